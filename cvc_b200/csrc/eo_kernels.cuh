@@ -1,0 +1,310 @@
+// Even/odd (Schur-complement) stencil and vector kernels for the batched
+// solver, templated on the storage of spinors and links.
+//
+// With Q = A + (-1/2) H, A = 1/(2 kappa) + i mu g5 (site-diagonal) and H the
+// hopping sum, the odd-site Schur complement is
+//   M = A_oo - 1/4 H_oe A_ee^-1 H_eo,   M(mu)^+ = g5 M(-mu) g5,
+// and one application of M^+ M is four half-lattice stencil sweeps of the
+// single kernel k_eo_hop:
+//   out_p = D2 aux_p + D1 ( c [g5] H_pq ([g5] in_q) )
+// with D1, D2 site-diagonal operators alpha + i beta g5.
+//
+// Thread mapping: x = site within the output parity, y = right-hand side.
+// The y-threads of one block handle different right-hand sides of the same
+// sites, so each link is fetched from HBM once and served from L1 to the
+// others ("multi-RHS": link traffic / N).
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include "cvcb_internal.h"
+#include "spinor_ops.cuh"
+
+namespace cvcb {
+
+// ---- spinor storage accessors ---------------------------------------------
+// Element (rhs r, site j) of a field set; `stride` separates the complex
+// components (SoA), `rstride` separates right-hand sides.
+struct F64Acc {
+  using R = double;
+  double2 *p;
+  size_t stride, rstride;
+  __device__ __forceinline__ Spinor<double> load(int r, int j) const {
+    return load_spinor(p + r * rstride, stride, j);
+  }
+  __device__ __forceinline__ void store(int r, int j, const Spinor<double> &s) const {
+    store_spinor(p + r * rstride, stride, j, s);
+  }
+};
+
+struct F32Acc {
+  using R = float;
+  float4 *p;
+  size_t stride, rstride;
+  __device__ __forceinline__ Spinor<float> load(int r, int j) const {
+    const float4 *q = p + r * rstride + j;
+    Spinor<float> s;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float4 v = __ldg(q + k * stride);
+      s.c[(2 * k) / 3][(2 * k) % 3] = cx(v.x, v.y);
+      s.c[(2 * k + 1) / 3][(2 * k + 1) % 3] = cx(v.z, v.w);
+    }
+    return s;
+  }
+  __device__ __forceinline__ void store(int r, int j, const Spinor<float> &s) const {
+    float4 *q = p + r * rstride + j;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const Cx<float> a = s.c[(2 * k) / 3][(2 * k) % 3], b = s.c[(2 * k + 1) / 3][(2 * k + 1) % 3];
+      q[k * stride] = make_float4(a.re, a.im, b.re, b.im);
+    }
+  }
+};
+
+// FP16 with one float scale per site: value = half * norm, |half| <= 1.
+struct F16Acc {
+  using R = float;
+  uint4 *p;
+  float *norm;
+  size_t stride, rstride;
+  __device__ __forceinline__ Spinor<float> load(int r, int j) const {
+    const uint4 *q = p + r * rstride + j;
+    const float nm = __ldg(norm + r * stride + j);
+    Spinor<float> s;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const uint4 v = __ldg(q + k * stride);
+      const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w[m]));
+        const int c = 4 * k + m;
+        s.c[c / 3][c % 3] = cx(f.x * nm, f.y * nm);
+      }
+    }
+    return s;
+  }
+  __device__ __forceinline__ void store(int r, int j, const Spinor<float> &s) const {
+    float mx = 0.f;
+#pragma unroll
+    for (int c = 0; c < 12; ++c)
+      mx = fmaxf(mx, fmaxf(fabsf(s.c[c / 3][c % 3].re), fabsf(s.c[c / 3][c % 3].im)));
+    const float inv = mx > 0.f ? 1.f / mx : 0.f;
+    uint4 *q = p + r * rstride + j;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      unsigned w[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int c = 4 * k + m;
+        __half2 h = __floats2half2_rn(s.c[c / 3][c % 3].re * inv, s.c[c / 3][c % 3].im * inv);
+        w[m] = *reinterpret_cast<unsigned *>(&h);
+      }
+      q[k * stride] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    norm[r * stride + j] = mx;
+  }
+};
+
+// ---- link accessors ---------------------------------------------------------
+// kPhased: the stored link already carries the boundary phase.  Otherwise the
+// raw SU(3) link is rebuilt from two rows and the phase is applied to the
+// product U h (forward) or U^+ h (backward, conjugate phase).
+struct L64 {
+  using R = double;
+  static constexpr bool kPhased = true;
+  const double2 *U;
+  size_t V;
+  double2 ph[4];
+  __device__ __forceinline__ Link<double> load(int mu, int j) const { return load_link64(U, V, mu, j); }
+};
+
+struct L32f {  // 18 reals, single, phased
+  using R = float;
+  static constexpr bool kPhased = true;
+  const float2 *U;
+  size_t V;
+  float2 ph[4];
+  __device__ __forceinline__ Link<float> load(int mu, int j) const {
+    Link<float> L;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float2 v = __ldg(U + (size_t)(mu * 9 + k) * V + j);
+      L.m[k / 3][k % 3] = cx(v.x, v.y);
+    }
+    return L;
+  }
+};
+
+struct L32c {  // 12 reals, single, raw SU(3)
+  using R = float;
+  static constexpr bool kPhased = false;
+  const float4 *U;
+  size_t V;
+  float2 ph[4];
+  __device__ __forceinline__ Link<float> load(int mu, int j) const {
+    Link<float> L;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const float4 v = __ldg(U + (size_t)(mu * 3 + q) * V + j);
+      L.m[(2 * q) / 3][(2 * q) % 3] = cx(v.x, v.y);
+      L.m[(2 * q + 1) / 3][(2 * q + 1) % 3] = cx(v.z, v.w);
+    }
+    reconstruct_row2(L);
+    return L;
+  }
+};
+
+struct L16c {  // 12 reals, half, raw SU(3)
+  using R = float;
+  static constexpr bool kPhased = false;
+  const uint2 *U;
+  size_t V;
+  float2 ph[4];
+  __device__ __forceinline__ Link<float> load(int mu, int j) const {
+    Link<float> L;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const uint2 v = __ldg(U + (size_t)(mu * 3 + q) * V + j);
+      const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&v.x));
+      const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&v.y));
+      L.m[(2 * q) / 3][(2 * q) % 3] = cx(a.x, a.y);
+      L.m[(2 * q + 1) / 3][(2 * q + 1) % 3] = cx(b.x, b.y);
+    }
+    reconstruct_row2(L);
+    return L;
+  }
+};
+
+template <typename R>
+__device__ __forceinline__ Cx<R> to_cx(double2 v) {
+  return cx((R)v.x, (R)v.y);
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> to_cx(float2 v) {
+  return cx((R)v.x, (R)v.y);
+}
+
+template <typename R>
+__device__ __forceinline__ HalfSpinor<R> cscale(const HalfSpinor<R> &h, Cx<R> z) {
+  HalfSpinor<R> o;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.c[a][c] = cmul(h.c[a][c], z);
+  return o;
+}
+
+// out = (alpha + i beta g5) v
+template <typename R>
+__device__ __forceinline__ Spinor<R> diag_op(R alpha, R beta, const Spinor<R> &v) {
+  Spinor<R> o;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const R b = s < 2 ? beta : -beta;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const Cx<R> x = v.c[s][c];
+      o.c[s][c] = cx(alpha * x.re - b * x.im, alpha * x.im + b * x.re);
+    }
+  }
+  return o;
+}
+
+template <typename R>
+__device__ __forceinline__ void g5_inplace(Spinor<R> &v) {
+#pragma unroll
+  for (int s = 2; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v.c[s][c] = cx(-v.c[s][c].re, -v.c[s][c].im);
+}
+
+struct EoGeom {
+  Geom g;
+  int p;  // output parity
+};
+
+// Per-call arguments of the stencil kernel.
+template <class SF, class LF>
+struct HopArgs {
+  SF out, in, aux;
+  LF links;
+  EoGeom eg;
+  int nrhs;
+  const int *done;  // per right-hand side, may be null
+  double d1a, d1b;  // D1 = d1a + i d1b g5
+  double d2a, d2b;  // D2 = d2a + i d2b g5
+  double c;         // hop coefficient
+};
+
+// Grid: blockIdx.x = group of right-hand sides (fastest), blockIdx.y (and a
+// stride loop) = block of sites.  Blocks that run back to back therefore
+// share their sites, and a link fetched for one group of right-hand sides
+// is still in L2 (or L1) for the next.
+constexpr int kHopMaxThreads = 256;
+
+template <class SF, class LF, bool G5IN, bool G5HOP, bool AUX>
+__global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop(HopArgs<SF, LF> A) {
+  using R = typename SF::R;
+  const int r = blockIdx.x * blockDim.y + threadIdx.y;
+  const Geom &g = A.eg.g;
+  if (r >= A.nrhs) return;
+  if (A.done && A.done[r]) return;
+  for (int sb = blockIdx.y; sb * (int)blockDim.x < g.Vh; sb += gridDim.y) {
+  const int i = sb * blockDim.x + threadIdx.x;
+  if (i >= g.Vh) return;
+  const int p = A.eg.p;
+  const SiteCoord cd = site_coord(g, p, i);
+  const int self = p * g.Vh + i;  // link index of this site (links are full-lattice)
+  const int qoff = (1 - p) * g.Vh;
+
+  Spinor<R> acc;
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc.c[s][c] = cx((R)0, (R)0);
+
+#pragma unroll
+  for (int mu = 0; mu < 4; ++mu) {
+    {  // backward
+      const int j = nb_lex(g, cd, mu, -1) >> 1;
+      Spinor<R> f = A.in.load(r, j);
+      if (G5IN) g5_inplace(f);
+      const HalfSpinor<R> h = project(mu, +1, f);
+      const Link<R> W = A.links.load(mu, qoff + j);
+      HalfSpinor<R> u = link_dag_mul(W, h);
+      if (!LF::kPhased) u = cscale(u, cx((R)A.links.ph[mu].x, (R)-A.links.ph[mu].y));
+      accum_recon(mu, +1, acc, u);
+    }
+    {  // forward
+      const int j = nb_lex(g, cd, mu, +1) >> 1;
+      Spinor<R> f = A.in.load(r, j);
+      if (G5IN) g5_inplace(f);
+      const HalfSpinor<R> h = project(mu, -1, f);
+      const Link<R> W = A.links.load(mu, self);
+      HalfSpinor<R> u = link_mul(W, h);
+      if (!LF::kPhased) u = cscale(u, cx((R)A.links.ph[mu].x, (R)A.links.ph[mu].y));
+      accum_recon(mu, -1, acc, u);
+    }
+  }
+  if (G5HOP) g5_inplace(acc);
+  Spinor<R> o;
+  const R c = (R)A.c;
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) o.c[s][k] = c * acc.c[s][k];
+  o = diag_op((R)A.d1a, (R)A.d1b, o);
+  if (AUX) {
+    const Spinor<R> x = diag_op((R)A.d2a, (R)A.d2b, A.aux.load(r, i));
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) o.c[s][k] = o.c[s][k] + x.c[s][k];
+  }
+  A.out.store(r, i, o);
+  }
+}
+
+}  // namespace cvcb

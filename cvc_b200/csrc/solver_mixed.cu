@@ -1,0 +1,912 @@
+// Batched even/odd preconditioned CG on the normal equations of the Schur
+// complement, with reduced-precision inner iterations and FP64 reliable
+// updates.  Solves Q x_i = b_i for N right-hand sides per launch; Q is the
+// operator of Q_phi_tbc (Q_phi.c:38-188).  No counterpart in the reference,
+// which obtains propagators from files or from tmLQCD
+// (cvc_exact2_xspace.c:401-547).
+//
+// Per right-hand side (all kept on the device, one slot per rhs):
+//   b_hat = b_o + 1/2 H_oe A_ee^-1 b_e,  b_N = M^+ b_hat
+//   CG on M^+ M x_o = b_N in sloppy precision (FP32 or FP16+norm spinors,
+//   12-real or 18-real links); every time the sloppy residual has fallen by
+//   `delta` (or the residual estimate reaches the target) the FP64 solution
+//   absorbs the sloppy one and the true residuals r_hat = b_hat - M x and
+//   r_N = M^+ r_hat are recomputed in FP64 with the exact 18-real operator.
+//   |r_hat| is the residual of the full system (the even rows vanish by
+//   construction), so convergence is decided on |b - Q x| / |b| in FP64.
+//   Finally x_e = A_ee^-1 (b_e + 1/2 H_eo x_o) and |b - Q x| is checked with
+//   the full-lattice FP64 operator.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <tuple>
+#include <vector>
+
+#include "cvcb_internal.h"
+#include "eo_kernels.cuh"
+#include "reduce.cuh"
+
+namespace cvcb {
+
+namespace {
+
+constexpr int kMaxBatch = 24;
+
+// ---- batched reductions: blockIdx.y = right-hand side ----------------------
+struct BatchRed {
+  double *partials;    // [rhs][block]
+  unsigned *counters;  // [rhs]
+};
+
+template <class F, class E>
+__global__ void __launch_bounds__(kRedThreads)
+    k_reduce_rhs(F f, E e, int nsites, BatchRed br, const int *__restrict__ skip) {
+  const int r = blockIdx.y;
+  if (skip && skip[r]) return;
+  __shared__ double sh[1][kRedThreads / 32];
+  __shared__ bool last;
+  double v[1] = {0.0};
+  for (int s = blockIdx.x * kRedThreads + threadIdx.x; s < nsites; s += gridDim.x * kRedThreads)
+    v[0] += f(r, s);
+  block_sum<1>(v, sh);
+  double *part = br.partials + (size_t)r * kMaxRedBlocks;
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = v[0];
+    __threadfence();
+    last = atomicAdd(br.counters + r, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  v[0] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += kRedThreads) v[0] += __ldcg(part + b);
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) {
+    br.counters[r] = 0;
+    e(r, v[0]);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ double norm2(const Spinor<R> &a) {
+  double s = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) s += (double)a.c[k][c].re * a.c[k][c].re + (double)a.c[k][c].im * a.c[k][c].im;
+  return s;
+}
+template <typename R>
+__device__ __forceinline__ double redot(const Spinor<R> &a, const Spinor<R> &b) {
+  double s = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      s += (double)a.c[k][c].re * b.c[k][c].re + (double)a.c[k][c].im * b.c[k][c].im;
+  return s;
+}
+template <typename R, typename S>
+__device__ __forceinline__ Spinor<R> convert(const Spinor<S> &a) {
+  Spinor<R> o;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.c[k][c] = cx((R)a.c[k][c].re, (R)a.c[k][c].im);
+  return o;
+}
+
+struct Scal {  // per right-hand side, device arrays
+  double *rr, *pAp, *alpha, *beta, *rhat2, *rn2;
+  int *done;
+};
+
+// pAp = Re <p, Ap>; alpha = rr / pAp
+template <class SF>
+struct RedPAp {
+  SF p, Ap;
+  __device__ double operator()(int r, int s) const { return redot(p.load(r, s), Ap.load(r, s)); }
+};
+struct EpiAlphaB {
+  Scal S;
+  __device__ void operator()(int r, double t) const {
+    S.pAp[r] = t;
+    // M^+ M is positive definite; a non-positive <p, M^+ M p> only comes from
+    // rounding at the end of convergence: take no step and let the host's
+    // reliable update refresh the residual.
+    S.alpha[r] = (t > 0 && isfinite(t)) ? S.rr[r] / t : 0.0;
+  }
+};
+
+// x_s += alpha p; r_s -= alpha Ap; rr_new = |r_s|^2; beta = rr_new / rr
+template <class SF, class XF>
+struct RedUpdate {
+  SF p, Ap, rs;
+  XF xs;
+  Scal S;
+  __device__ double operator()(int r, int s) const {
+    using R = typename SF::R;
+    using RX = typename XF::R;
+    const double a = S.alpha[r];
+    const Spinor<R> pv = p.load(r, s), apv = Ap.load(r, s);
+    Spinor<R> rv = rs.load(r, s);
+    Spinor<RX> xv = xs.load(r, s);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        xv.c[k][c].re += (RX)(a * pv.c[k][c].re);
+        xv.c[k][c].im += (RX)(a * pv.c[k][c].im);
+        rv.c[k][c].re -= (R)(a * apv.c[k][c].re);
+        rv.c[k][c].im -= (R)(a * apv.c[k][c].im);
+      }
+    xs.store(r, s, xv);
+    rs.store(r, s, rv);
+    return norm2(rv);
+  }
+};
+struct EpiBetaB {
+  Scal S;
+  __device__ void operator()(int r, double t) const {
+    S.beta[r] = t / S.rr[r];
+    S.rr[r] = t;
+  }
+};
+
+// p = r_s + beta p
+template <class SF>
+__global__ void k_p_upd(SF p, SF rs, Scal S, int nsites, int nrhs) {
+  using R = typename SF::R;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (s >= nsites || r >= nrhs || S.done[r]) return;
+  const R b = (R)S.beta[r];
+  const Spinor<R> rv = rs.load(r, s);
+  Spinor<R> pv = p.load(r, s);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pv.c[k][c] = rv.c[k][c] + b * pv.c[k][c];
+  p.store(r, s, pv);
+}
+
+// Reliable update, step 1: x64 += x_s; x_s = 0 (rhs with skip[r] == 0)
+template <class XF>
+__global__ void k_absorb(F64Acc x64, XF xs, const int *skip, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (s >= nsites || r >= nrhs || skip[r]) return;
+  using RX = typename XF::R;
+  Spinor<double> xv = x64.load(r, s);
+  const Spinor<RX> d = xs.load(r, s);
+  Spinor<RX> z;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      xv.c[k][c].re += (double)d.c[k][c].re;
+      xv.c[k][c].im += (double)d.c[k][c].im;
+      z.c[k][c] = cx((RX)0, (RX)0);
+    }
+  x64.store(r, s, xv);
+  xs.store(r, s, z);
+}
+
+// r_hat = b_hat - y; returns |r_hat|^2
+struct RedRhat {
+  F64Acc bhat, y;
+  __device__ double operator()(int r, int s) const {
+    const Spinor<double> b = bhat.load(r, s);
+    Spinor<double> v = y.load(r, s);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v.c[k][c] = b.c[k][c] - v.c[k][c];
+    y.store(r, s, v);
+    return norm2(v);
+  }
+};
+struct EpiStore {
+  double *dst;
+  __device__ void operator()(int r, double t) const { dst[r] = t; }
+};
+
+// r_s = sloppy(r_N); returns |r_N|^2 (FP64)
+template <class SF>
+struct RedToSloppy {
+  F64Acc rN;
+  SF rs;
+  __device__ double operator()(int r, int s) const {
+    const Spinor<double> v = rN.load(r, s);
+    rs.store(r, s, convert<typename SF::R>(v));
+    return norm2(v);
+  }
+};
+struct EpiRR {
+  Scal S;
+  __device__ void operator()(int r, double t) const {
+    S.rr[r] = t;
+    S.rn2[r] = t;
+  }
+};
+
+// copy r_s into p (restart of the direction)
+template <class SF>
+__global__ void k_copy(SF dst, SF src, const int *skip, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (s >= nsites || r >= nrhs || (skip && skip[r])) return;
+  dst.store(r, s, src.load(r, s));
+}
+
+// t = D v (site-diagonal), FP64 fields
+__global__ void k_diag64(F64Acc out, F64Acc in, double a, double b, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (s >= nsites || r >= nrhs) return;
+  out.store(r, s, diag_op(a, b, in.load(r, s)));
+}
+
+// |v|^2 over the full lattice (both halves), FP64
+struct RedNorm64 {
+  F64Acc v;
+  __device__ double operator()(int r, int s) const { return norm2(v.load(r, s)); }
+};
+
+// y = a - b on full fields
+struct RedResid {
+  F64Acc a, b;
+  __device__ double operator()(int r, int s) const {
+    const Spinor<double> u = a.load(r, s), v = b.load(r, s);
+    double t = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double dr = u.c[k][c].re - v.c[k][c].re, di = u.c[k][c].im - v.c[k][c].im;
+        t += dr * dr + di * di;
+      }
+    return t;
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// The solver object for one batch
+// ---------------------------------------------------------------------------
+struct LaunchShape {
+  int bx = 64, by = 1;
+};
+
+// Autotuner results, per process: (V, precision, recon, n) -> launch shape,
+// (V, precision, recon, total rhs) -> right-hand sides per batch.
+std::map<std::tuple<int, int, int, int>, LaunchShape> g_tuned_shape;
+std::map<std::tuple<int, int, int, int>, int> g_tuned_batch;
+
+namespace {
+
+int red_blocks_sites(int n) {
+  int b = (n + kRedThreads * 2 - 1) / (kRedThreads * 2);
+  return std::max(1, std::min(b, kMaxRedBlocks));
+}
+
+template <class SF, class XF, class LF>
+struct Batch {
+  cvcb_lattice *L;
+  int n;  // rhs in this batch
+  Geom g;
+  LaunchShape shape;
+  // FP64 fields: full lattice, stride V, rhs stride 12V
+  double2 *b64, *x64, *t64, *y64, *bh64, *rn64;
+  // sloppy fields: half lattice, compact
+  SF p, Ap, rs, te, yo, te2;
+  XF xs;
+  void *xs_mem;
+  size_t xs_bytes;
+  Scal S;
+  int *ru_skip;  // per rhs: 1 = skip in the reliable update
+  BatchRed br;
+  LF links;
+  L64 links64;
+  double mu, kap;
+
+  F64Acc f64(double2 *base, int parity) const {
+    return F64Acc{base + (size_t)parity * g.Vh, (size_t)g.V, (size_t)12 * g.V};
+  }
+  F64Acc f64full(double2 *base) const { return F64Acc{base, (size_t)g.V, (size_t)12 * g.V}; }
+
+  template <class AF, class LL, bool G5IN, bool G5HOP, bool AUX>
+  int hop(AF out, AF in, AF aux, LL lk, int parity, const int *done, double d1a, double d1b,
+          double d2a, double d2b, double c) {
+    HopArgs<AF, LL> a{out, in, aux, lk, EoGeom{g, parity}, n, done, d1a, d1b, d2a, d2b, c};
+    // FP64 sweeps (reliable updates) always use a fixed small shape
+    const LaunchShape sh = sizeof(typename AF::R) == 8 && sizeof(typename SF::R) != 8
+                               ? LaunchShape{64, 1} : shape;
+    const int by = std::min(sh.by, n);
+    const int site_blocks = (g.Vh + sh.bx - 1) / sh.bx;
+    dim3 block(sh.bx, by), grid((n + by - 1) / by, std::min(site_blocks, 65535));
+    k_eo_hop<AF, LL, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
+    CVCB_CUDA(cudaGetLastError());
+    return CVCB_OK;
+  }
+
+  // diagonal coefficients
+  double ka() const { return 0.5 / kap; }
+  void ainv(double m, double &a, double &b) const {
+    const double d = ka() * ka() + m * m;
+    a = ka() / d;
+    b = -m / d;
+  }
+
+  // out_o = M^+ M in_o with sloppy fields (te, yo, te2 as intermediates)
+  int normal_op_sloppy(SF out, SF in, const int *done) {
+    double ia, ib, ja, jb;
+    ainv(mu, ia, ib);
+    ainv(-mu, ja, jb);
+    // K1: te = A^-1(mu) (-1/2 H_eo in)
+    CVCB_TRY((hop<SF, LF, false, false, false>(te, in, in, links, 0, done, ia, ib, 0, 0, -0.5)));
+    // K2: yo = A(mu) in + 1/2 H_oe te
+    CVCB_TRY((hop<SF, LF, false, false, true>(yo, te, in, links, 1, done, 1, 0, ka(), mu, 0.5)));
+    // K1': te2 = A^-1(-mu) (-1/2 H_eo g5 yo)
+    CVCB_TRY((hop<SF, LF, true, false, false>(te2, yo, yo, links, 0, done, ja, jb, 0, 0, -0.5)));
+    // K2': out = A(-mu) yo + 1/2 g5 H_oe te2
+    return hop<SF, LF, false, true, true>(out, te2, yo, links, 1, done, 1, 0, ka(), -mu, 0.5);
+  }
+
+  // one CG iteration (sloppy)
+  int iteration() {
+    CVCB_TRY(normal_op_sloppy(Ap, p, S.done));
+    dim3 rg(red_blocks_sites(g.Vh), n);
+    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedPAp<SF>{p, Ap}, EpiAlphaB{S}, g.Vh, br,
+                                                    S.done);
+    CVCB_CUDA(cudaGetLastError());
+    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedUpdate<SF, XF>{p, Ap, rs, xs, S},
+                                                    EpiBetaB{S}, g.Vh, br, S.done);
+    CVCB_CUDA(cudaGetLastError());
+    dim3 eg((g.Vh + 127) / 128, n);
+    k_p_upd<<<eg, 128, 0, L->stream>>>(p, rs, S, g.Vh, n);
+    CVCB_CUDA(cudaGetLastError());
+    return CVCB_OK;
+  }
+
+  // FP64: out_o = M(m) in_o  (t64 even half as intermediate)
+  int schur64(double2 *out, double2 *in, double m, const int *skip) {
+    double ia, ib;
+    ainv(m, ia, ib);
+    CVCB_TRY((hop<F64Acc, L64, false, false, false>(f64(t64, 0), f64(in, 1), f64(in, 1), links64, 0,
+                                                    skip, ia, ib, 0, 0, -0.5)));
+    return hop<F64Acc, L64, false, false, true>(f64(out, 1), f64(t64, 0), f64(in, 1), links64, 1,
+                                                skip, 1, 0, ka(), m, 0.5);
+  }
+  // FP64: out_o = M(mu)^+ in_o = g5 M(-mu) g5 in_o
+  int schur64_dag(double2 *out, double2 *in, const int *skip) {
+    double ia, ib;
+    ainv(-mu, ia, ib);
+    CVCB_TRY((hop<F64Acc, L64, true, false, false>(f64(t64, 0), f64(in, 1), f64(in, 1), links64, 0,
+                                                   skip, ia, ib, 0, 0, -0.5)));
+    return hop<F64Acc, L64, false, true, true>(f64(out, 1), f64(t64, 0), f64(in, 1), links64, 1,
+                                               skip, 1, 0, ka(), -mu, 0.5);
+  }
+
+  // r_hat = b_hat - M x64; rhat2 = |r_hat|^2; r_N = M^+ r_hat; r_s = r_N; rr = |r_N|^2
+  int reliable_update(bool absorb) {
+    dim3 eg((g.Vh + 127) / 128, n);
+    if (absorb) {
+      k_absorb<<<eg, 128, 0, L->stream>>>(f64(x64, 1), xs, ru_skip, g.Vh, n);
+      CVCB_CUDA(cudaGetLastError());
+    }
+    CVCB_TRY(schur64(y64, x64, mu, ru_skip));
+    dim3 rg(red_blocks_sites(g.Vh), n);
+    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedRhat{f64(bh64, 1), f64(y64, 1)},
+                                                    EpiStore{S.rhat2}, g.Vh, br, ru_skip);
+    CVCB_CUDA(cudaGetLastError());
+    CVCB_TRY(schur64_dag(rn64, y64, ru_skip));
+    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedToSloppy<SF>{f64(rn64, 1), rs}, EpiRR{S},
+                                                    g.Vh, br, ru_skip);
+    CVCB_CUDA(cudaGetLastError());
+    return CVCB_OK;
+  }
+};
+
+template <class SF>
+SF make_sloppy(void *base, size_t Vh, int r_count, float *norm_base);
+
+template <>
+F32Acc make_sloppy<F32Acc>(void *base, size_t Vh, int, float *) {
+  return F32Acc{static_cast<float4 *>(base), Vh, 6 * Vh};
+}
+template <>
+F16Acc make_sloppy<F16Acc>(void *base, size_t Vh, int, float *norm) {
+  return F16Acc{static_cast<uint4 *>(base), norm, Vh, 3 * Vh};
+}
+template <>
+F64Acc make_sloppy<F64Acc>(void *base, size_t Vh, int, float *) {
+  return F64Acc{static_cast<double2 *>(base), Vh, 12 * Vh};
+}
+
+template <class SF>
+size_t sloppy_site_bytes();
+template <>
+size_t sloppy_site_bytes<F32Acc>() { return 96; }
+template <>
+size_t sloppy_site_bytes<F16Acc>() { return 48; }
+template <>
+size_t sloppy_site_bytes<F64Acc>() { return 192; }
+
+template <class LF>
+LF make_links(cvcb_lattice *L);
+template <>
+L64 make_links<L64>(cvcb_lattice *L) {
+  L64 l{L->U64, (size_t)L->g.V, {}};
+  for (int m = 0; m < 4; ++m) l.ph[m] = make_double2(L->phase[2 * m], L->phase[2 * m + 1]);
+  return l;
+}
+template <>
+L32c make_links<L32c>(cvcb_lattice *L) {
+  L32c l{L->U32c, (size_t)L->g.V, {}};
+  for (int m = 0; m < 4; ++m) l.ph[m] = make_float2((float)L->phase[2 * m], (float)L->phase[2 * m + 1]);
+  return l;
+}
+template <>
+L32f make_links<L32f>(cvcb_lattice *L) {
+  L32f l{L->U32f, (size_t)L->g.V, {}};
+  for (int m = 0; m < 4; ++m) l.ph[m] = make_float2((float)L->phase[2 * m], (float)L->phase[2 * m + 1]);
+  return l;
+}
+template <>
+L16c make_links<L16c>(cvcb_lattice *L) {
+  L16c l{L->U16c, (size_t)L->g.V, {}};
+  for (int m = 0; m < 4; ++m) l.ph[m] = make_float2((float)L->phase[2 * m], (float)L->phase[2 * m + 1]);
+  return l;
+}
+
+// Device memory of one batch of n right-hand sides.
+struct BatchMem {
+  size_t f64_bytes, sl_bytes, norm_bytes;
+  char *base = nullptr;
+};
+
+template <class SF, class XF, class LF>
+int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n) {
+  const Geom &g = L->g;
+  B.L = L;
+  B.n = n;
+  B.g = g;
+  B.mu = L->mu;
+  B.kap = L->kappa;
+  B.links = make_links<LF>(L);
+  B.links64 = make_links<L64>(L);
+  const size_t f64 = (size_t)12 * g.V * sizeof(double2) * n;  // one FP64 full field set
+  const size_t sl = sloppy_site_bytes<SF>() * (size_t)g.Vh * n;
+  const size_t xsl = sloppy_site_bytes<XF>() * (size_t)g.Vh * n;
+  const size_t nrm = sizeof(float) * (size_t)g.Vh * n;
+  const size_t scal = (6 * sizeof(double) + 2 * sizeof(int)) * kMaxBatch + 64;
+  const size_t part = sizeof(double) * kMaxRedBlocks * kMaxBatch + sizeof(unsigned) * kMaxBatch;
+  const size_t total = 6 * f64 + 6 * (sl + nrm) + (xsl + nrm) + scal + part + 4096;
+  void *mem;
+  CVCB_TRY(ensure_buffer(L, SLOT_MIX0, total, &mem));
+  char *p = static_cast<char *>(mem);
+  auto take = [&](size_t bytes) {
+    char *q = p;
+    p += (bytes + 255) & ~size_t(255);
+    return q;
+  };
+  B.b64 = (double2 *)take(f64);
+  B.x64 = (double2 *)take(f64);
+  B.t64 = (double2 *)take(f64);
+  B.y64 = (double2 *)take(f64);
+  B.bh64 = (double2 *)take(f64);
+  B.rn64 = (double2 *)take(f64);
+  SF *sl_fields[6] = {&B.p, &B.Ap, &B.rs, &B.te, &B.yo, &B.te2};
+  for (SF *f : sl_fields) {
+    void *b = take(sl);
+    float *nb = (float *)take(nrm);
+    *f = make_sloppy<SF>(b, g.Vh, n, nb);
+  }
+  {
+    void *b = take(xsl);
+    float *nb = (float *)take(nrm);
+    B.xs = make_sloppy<XF>(b, g.Vh, n, nb);
+    B.xs_mem = b;
+    B.xs_bytes = xsl;
+  }
+  B.S.rr = (double *)take(sizeof(double) * kMaxBatch);
+  B.S.pAp = (double *)take(sizeof(double) * kMaxBatch);
+  B.S.alpha = (double *)take(sizeof(double) * kMaxBatch);
+  B.S.beta = (double *)take(sizeof(double) * kMaxBatch);
+  B.S.rhat2 = (double *)take(sizeof(double) * kMaxBatch);
+  B.S.rn2 = (double *)take(sizeof(double) * kMaxBatch);
+  B.S.done = (int *)take(sizeof(int) * kMaxBatch);
+  B.ru_skip = (int *)take(sizeof(int) * kMaxBatch);
+  B.br.partials = (double *)take(sizeof(double) * kMaxRedBlocks * kMaxBatch);
+  B.br.counters = (unsigned *)take(sizeof(unsigned) * kMaxBatch);
+  CVCB_CUDA(cudaMemsetAsync(B.br.counters, 0, sizeof(unsigned) * kMaxBatch, L->stream));
+  CVCB_CUDA(cudaMemsetAsync(B.S.done, 0, sizeof(int) * kMaxBatch, L->stream));
+  CVCB_CUDA(cudaMemsetAsync(B.ru_skip, 0, sizeof(int) * kMaxBatch, L->stream));
+  return CVCB_OK;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Times `fn` (which enqueues work on L->stream) with CUDA events, best of reps.
+template <class Fn>
+int time_ms(cvcb_lattice *L, Fn fn, int reps, float *best) {
+  cudaEvent_t a, b;
+  CVCB_CUDA(cudaEventCreate(&a));
+  CVCB_CUDA(cudaEventCreate(&b));
+  *best = 1e30f;
+  for (int i = 0; i < reps; ++i) {
+    CVCB_CUDA(cudaEventRecord(a, L->stream));
+    CVCB_TRY(fn());
+    CVCB_CUDA(cudaEventRecord(b, L->stream));
+    CVCB_CUDA(cudaEventSynchronize(b));
+    float ms;
+    CVCB_CUDA(cudaEventElapsedTime(&ms, a, b));
+    *best = std::min(*best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return CVCB_OK;
+}
+
+// Autotuner for the stencil launch shape: sites per block x right-hand sides
+// per block, timed on the sloppy normal operator.
+template <class SF, class XF, class LF>
+int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon) {
+  auto key = std::make_tuple(L->g.V, prec, recon, B.n);
+  auto it = g_tuned_shape.find(key);
+  if (it != g_tuned_shape.end()) {
+    B.shape = it->second;
+    return CVCB_OK;
+  }
+  LaunchShape best;
+  float best_ms = 1e30f;
+  const int bxs[] = {32, 64, 128, 256};
+  const int bys[] = {1, 2, 4, 8, 12};
+  for (int bx : bxs)
+    for (int by : bys) {
+      if (by > B.n || bx * by > kHopMaxThreads || bx * by < 32) continue;
+      B.shape.bx = bx;
+      B.shape.by = by;
+      float ms;
+      if (time_ms(L, [&] { return B.normal_op_sloppy(B.Ap, B.p, nullptr); }, 3, &ms) != CVCB_OK) {
+        cudaGetLastError();
+        continue;
+      }
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = B.shape;
+      }
+    }
+  B.shape = best;
+  g_tuned_shape[key] = best;
+  return CVCB_OK;
+}
+
+template <class SF, class XF, class LF>
+int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
+              const cvcb_solver_params *P, cvcb_solver_stats *st, LaunchShape *shape_out) {
+  Batch<SF, XF, LF> B;
+  CVCB_TRY(setup_batch(L, B, n));
+  const Geom &g = L->g;
+  const size_t fs = (size_t)12 * g.V;
+  dim3 eg((g.Vh + 127) / 128, n);
+  dim3 egf((g.V + 127) / 128, n);
+  dim3 rg(red_blocks_sites(g.Vh), n), rgf(red_blocks_sites(g.V), n);
+
+  for (int i = 0; i < n; ++i) CVCB_TRY(spinor_in(L, B.b64 + i * fs, b[i], g.V));
+  CVCB_TRY(tune_shape(L, B, P->precision, P->link_recon));
+  if (shape_out) *shape_out = B.shape;
+
+  // |b|^2 over the full lattice
+  double *bnorm2 = B.S.rn2;  // temporary use
+  k_reduce_rhs<<<rgf, kRedThreads, 0, L->stream>>>(RedNorm64{B.f64full(B.b64)},
+                                                   EpiStore{bnorm2}, g.V, B.br, nullptr);
+  CVCB_CUDA(cudaGetLastError());
+  std::vector<double> hb2(n);
+  CVCB_CUDA(cudaMemcpyAsync(hb2.data(), bnorm2, n * sizeof(double), cudaMemcpyDeviceToHost,
+                            L->stream));
+  // b_hat = b_o + 1/2 H_oe A_ee^-1 b_e
+  double ia, ib;
+  B.ainv(B.mu, ia, ib);
+  k_diag64<<<eg, 128, 0, L->stream>>>(B.f64(B.t64, 0), B.f64(B.b64, 0), ia, ib, g.Vh, n);
+  CVCB_CUDA(cudaGetLastError());
+  CVCB_TRY((B.template hop<F64Acc, L64, false, false, true>(B.f64(B.bh64, 1), B.f64(B.t64, 0),
+                                                            B.f64(B.b64, 1), B.links64, 1,
+                                                            nullptr, 1, 0, 1, 0, 0.5)));
+  // x = 0, x_s = 0; reliable update from x = 0 gives r_hat = b_hat, r_N = b_N
+  CVCB_CUDA(cudaMemsetAsync(B.x64, 0, fs * n * sizeof(double2), L->stream));
+  CVCB_TRY(B.reliable_update(false));
+  // x_s = 0 (all-zero bits are 0.0), p = r_s
+  CVCB_CUDA(cudaMemsetAsync(B.xs_mem, 0, B.xs_bytes, L->stream));
+  k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, nullptr, g.Vh, n);
+  CVCB_CUDA(cudaGetLastError());
+  std::vector<double> rr(n), rr_max(n), rhat2(n), ratio2(n), target2(n);
+  std::vector<int> done(n, 0), iters(n, 0), since(n, 0), skip(n, 0);
+  CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+  CVCB_CUDA(cudaMemcpyAsync(rhat2.data(), B.S.rhat2, n * sizeof(double), cudaMemcpyDeviceToHost,
+                            L->stream));
+  CVCB_CUDA(cudaStreamSynchronize(L->stream));
+  const double margin = 0.5;
+  for (int i = 0; i < n; ++i) {
+    target2[i] = std::pow(P->tol * margin, 2) * hb2[i];
+    rr_max[i] = rr[i];
+    ratio2[i] = rhat2[i] > 0 ? rr[i] / rhat2[i] : 1.0;
+    if (!(hb2[i] > 0)) done[i] = 1;  // zero right-hand side: x = 0
+    else if (rhat2[i] <= target2[i]) done[i] = 1;
+  }
+  CVCB_CUDA(cudaMemcpyAsync(B.S.done, done.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                            L->stream));
+
+  // capture a chunk of iterations in a CUDA graph
+  const int chunk = 10;
+  cudaGraphExec_t gexec = nullptr;
+  if (P->use_graph) {
+    cudaGraph_t graph;
+    CVCB_CUDA(cudaStreamBeginCapture(L->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = CVCB_OK;
+    for (int k = 0; k < chunk && rc == CVCB_OK; ++k) rc = B.iteration();
+    cudaError_t ec = cudaStreamEndCapture(L->stream, &graph);
+    if (rc != CVCB_OK) return rc;
+    CVCB_CUDA(ec);
+    CVCB_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
+    cudaGraphDestroy(graph);
+  }
+
+  const double delta2 = P->delta * P->delta;
+  int total_iter = 0, nru = 0;
+  const double t0 = now_s();
+  int rc = CVCB_OK;
+  while (true) {
+    bool all = true;
+    for (int i = 0; i < n; ++i) all = all && done[i];
+    if (all) break;
+    if (total_iter >= P->max_iter) break;
+    if (gexec) {
+      cudaError_t e = cudaGraphLaunch(gexec, L->stream);
+      if (e != cudaSuccess) {
+        set_error("graph launch: %s", cudaGetErrorString(e));
+        rc = CVCB_ERR_CUDA;
+        break;
+      }
+    } else {
+      for (int k = 0; k < chunk; ++k)
+        if ((rc = B.iteration()) != CVCB_OK) break;
+      if (rc != CVCB_OK) break;
+    }
+    total_iter += chunk;
+    CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost,
+                              L->stream));
+    CVCB_CUDA(cudaStreamSynchronize(L->stream));
+    bool any = false;
+    for (int i = 0; i < n; ++i) {
+      skip[i] = 1;
+      if (done[i]) continue;
+      iters[i] += chunk;
+      since[i] += chunk;
+      const bool bad = !std::isfinite(rr[i]);
+      const bool dropped = rr[i] < delta2 * rr_max[i];
+      const bool near = rr[i] / ratio2[i] < target2[i];
+      if (bad || dropped || near || since[i] >= 1000) {
+        skip[i] = 0;
+        any = true;
+      }
+    }
+    if (!any) continue;
+    CVCB_CUDA(cudaMemcpyAsync(B.ru_skip, skip.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                              L->stream));
+    CVCB_TRY(B.reliable_update(true));
+    // restart the search direction of updated rhs from the true residual
+    k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.ru_skip, g.Vh, n);
+    CVCB_CUDA(cudaGetLastError());
+    ++nru;
+    CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost,
+                              L->stream));
+    CVCB_CUDA(cudaMemcpyAsync(rhat2.data(), B.S.rhat2, n * sizeof(double), cudaMemcpyDeviceToHost,
+                              L->stream));
+    CVCB_CUDA(cudaStreamSynchronize(L->stream));
+    for (int i = 0; i < n; ++i) {
+      if (skip[i]) continue;
+      since[i] = 0;
+      rr_max[i] = rr[i];
+      if (rhat2[i] > 0) ratio2[i] = rr[i] / rhat2[i];
+      if (rhat2[i] <= target2[i]) done[i] = 1;
+    }
+    CVCB_CUDA(cudaMemcpyAsync(B.S.done, done.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                              L->stream));
+  }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (rc != CVCB_OK) return rc;
+
+  // x_e = A^-1 (b_e + 1/2 H_eo x_o)
+  CVCB_TRY((B.template hop<F64Acc, L64, false, false, true>(B.f64(B.x64, 0), B.f64(B.x64, 1),
+                                                            B.f64(B.b64, 0), B.links64, 0,
+                                                            nullptr, ia, ib, ia, ib, 0.5)));
+  // final FP64 check |b - Q x| / |b| with the full-lattice operator
+  double worst = 0.0;
+  int nconv = 0;
+  for (int i = 0; i < n; ++i) {
+    CVCB_TRY(launch_tm_full(L, B.t64 + i * fs, B.x64 + i * fs, 0.5 / L->kappa, L->mu, -0.5, false,
+                            nullptr));
+  }
+  k_reduce_rhs<<<rgf, kRedThreads, 0, L->stream>>>(
+      RedResid{B.f64full(B.t64), B.f64full(B.b64)}, EpiStore{B.S.rhat2}, g.V, B.br, nullptr);
+  CVCB_CUDA(cudaGetLastError());
+  CVCB_CUDA(cudaMemcpyAsync(rhat2.data(), B.S.rhat2, n * sizeof(double), cudaMemcpyDeviceToHost,
+                            L->stream));
+  for (int i = 0; i < n; ++i) CVCB_TRY(spinor_out(L, x[i], B.x64 + i * fs, g.V));
+  CVCB_CUDA(cudaStreamSynchronize(L->stream));
+  for (int i = 0; i < n; ++i) {
+    const double rel = hb2[i] > 0 ? std::sqrt(rhat2[i] / hb2[i]) : 0.0;
+    worst = std::max(worst, rel);
+    if (rel <= P->tol) ++nconv;
+  }
+  st->iterations += std::accumulate(iters.begin(), iters.end(), 0);
+  st->reliable_updates += nru;
+  st->converged += nconv;
+  st->max_true_res = std::max(st->max_true_res, worst);
+  st->seconds += now_s() - t0;
+  return CVCB_OK;
+}
+
+template <class SF, class XF, class LF>
+int time_stencil_t(cvcb_lattice *L, int prec, int recon, int nrhs, int reps, double *ms) {
+  Batch<SF, XF, LF> B;
+  CVCB_TRY(setup_batch(L, B, nrhs));
+  // zero contents: timing of the stencil does not depend on the values
+  CVCB_CUDA(cudaMemsetAsync(B.p.p, 0, sloppy_site_bytes<SF>() * (size_t)L->g.Vh * nrhs, L->stream));
+  CVCB_CUDA(cudaMemsetAsync(B.S.done, 0, sizeof(int) * nrhs, L->stream));
+  CVCB_TRY(tune_shape(L, B, prec, recon));
+  double ia, ib;
+  B.ainv(B.mu, ia, ib);
+  auto one = [&] {
+    return B.template hop<SF, LF, false, false, false>(B.te, B.p, B.p, B.links, 0, nullptr, ia,
+                                                       ib, 0, 0, -0.5);
+  };
+  CVCB_TRY(one());
+  float best;
+  cudaEvent_t a, b;
+  CVCB_CUDA(cudaEventCreate(&a));
+  CVCB_CUDA(cudaEventCreate(&b));
+  CVCB_CUDA(cudaEventRecord(a, L->stream));
+  for (int i = 0; i < reps; ++i) CVCB_TRY(one());
+  CVCB_CUDA(cudaEventRecord(b, L->stream));
+  CVCB_CUDA(cudaEventSynchronize(b));
+  CVCB_CUDA(cudaEventElapsedTime(&best, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = best / reps;
+  return CVCB_OK;
+}
+
+}  // namespace
+
+int time_stencil(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int reps, double *ms) {
+  if (!L->have_gauge) {
+    set_error("no gauge field uploaded");
+    return CVCB_ERR_STATE;
+  }
+  if (reps <= 0 || nrhs <= 0 || nrhs > kMaxBatch) return CVCB_ERR_ARG;
+  if (kind == 0) {
+    const size_t fb = (size_t)L->g.V * 12 * sizeof(double2);
+    void *f0, *f1;
+    CVCB_TRY(ensure_buffer(L, SLOT_F0, fb, &f0));
+    CVCB_TRY(ensure_buffer(L, SLOT_F1, fb, &f1));
+    CVCB_CUDA(cudaMemsetAsync(f0, 0, fb, L->stream));
+    auto one = [&] {
+      return launch_tm_full(L, (double2 *)f1, (const double2 *)f0, 0.5 / L->kappa, L->mu, -0.5,
+                            false, nullptr);
+    };
+    CVCB_TRY(one());
+    cudaEvent_t a, b;
+    CVCB_CUDA(cudaEventCreate(&a));
+    CVCB_CUDA(cudaEventCreate(&b));
+    CVCB_CUDA(cudaEventRecord(a, L->stream));
+    for (int i = 0; i < reps; ++i) CVCB_TRY(one());
+    CVCB_CUDA(cudaEventRecord(b, L->stream));
+    CVCB_CUDA(cudaEventSynchronize(b));
+    float t;
+    CVCB_CUDA(cudaEventElapsedTime(&t, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = t / reps;
+    return CVCB_OK;
+  }
+  if (prec == CVCB_PREC_DOUBLE) return time_stencil_t<F64Acc, F64Acc, L64>(L, prec, 18, nrhs, reps, ms);
+  if (prec == CVCB_PREC_SINGLE)
+    return recon == 12 ? time_stencil_t<F32Acc, F32Acc, L32c>(L, prec, recon, nrhs, reps, ms)
+                       : time_stencil_t<F32Acc, F32Acc, L32f>(L, prec, recon, nrhs, reps, ms);
+  return recon == 12 ? time_stencil_t<F16Acc, F32Acc, L16c>(L, prec, recon, nrhs, reps, ms)
+                     : time_stencil_t<F16Acc, F32Acc, L32f>(L, prec, recon, nrhs, reps, ms);
+}
+
+int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int nrhs,
+                  const cvcb_solver_params *P, cvcb_solver_stats *st) {
+  if (!L->have_gauge) {
+    set_error("no gauge field uploaded");
+    return CVCB_ERR_STATE;
+  }
+  if (nrhs <= 0) return CVCB_OK;
+  if (P->precision < 0 || P->precision > 2 || (P->link_recon != 12 && P->link_recon != 18) ||
+      !(P->tol > 0) || !(P->delta > 0 && P->delta < 1) || P->max_iter <= 0 ||
+      P->block_rhs < 0 || P->block_rhs > kMaxBatch) {
+    set_error("invalid solver parameters");
+    return CVCB_ERR_ARG;
+  }
+  int recon = P->link_recon;
+  if (recon == 12 && !(L->unitarity >= 0 && L->unitarity < 1e-6)) recon = 18;  // not SU(3)
+  std::memset(st, 0, sizeof *st);
+  int nb = P->block_rhs ? P->block_rhs : std::min(nrhs, 12);
+  if (!P->block_rhs) {
+    auto key = std::make_tuple(L->g.V, P->precision, recon, nrhs);
+    auto it = g_tuned_batch.find(key);
+    if (it != g_tuned_batch.end()) nb = it->second;
+  }
+  for (int off = 0; off < nrhs; off += nb) {
+    const int n = std::min(nb, nrhs - off);
+    int rc;
+    if (P->precision == CVCB_PREC_DOUBLE)
+      rc = run_batch<F64Acc, F64Acc, L64>(L, x + off, b + off, n, P, st, nullptr);
+    else if (P->precision == CVCB_PREC_SINGLE)
+      rc = recon == 12 ? run_batch<F32Acc, F32Acc, L32c>(L, x + off, b + off, n, P, st, nullptr)
+                       : run_batch<F32Acc, F32Acc, L32f>(L, x + off, b + off, n, P, st, nullptr);
+    else
+      rc = recon == 12 ? run_batch<F16Acc, F32Acc, L16c>(L, x + off, b + off, n, P, st, nullptr)
+                       : run_batch<F16Acc, F32Acc, L32f>(L, x + off, b + off, n, P, st, nullptr);
+    if (rc < 0) return rc;
+  }
+  return st->converged == nrhs ? CVCB_OK : CVCB_NO_CONVERGENCE;
+}
+
+}  // namespace cvcb
+
+extern "C" {
+
+void cvcb_solver_defaults(cvcb_solver_params *p) {
+  if (!p) return;
+  p->precision = CVCB_PREC_SINGLE;
+  p->link_recon = 12;
+  p->block_rhs = 0;
+  p->block_threads = 0;
+  p->max_iter = 20000;
+  p->use_graph = 1;
+  p->tol = 1e-10;
+  p->delta = 0.1;
+}
+
+int cvcb_tuned_shape(cvcb_lattice *L, int precision, int link_recon, int nrhs, int *sites_per_block,
+                     int *rhs_per_block) {
+  if (!L || !sites_per_block || !rhs_per_block) return CVCB_ERR_NULL;
+  auto it = cvcb::g_tuned_shape.find(std::make_tuple(L->g.V, precision, link_recon, nrhs));
+  if (it == cvcb::g_tuned_shape.end()) {
+    cvcb::set_error("no tuned shape for this configuration yet");
+    return CVCB_ERR_STATE;
+  }
+  *sites_per_block = it->second.bx;
+  *rhs_per_block = it->second.by;
+  return CVCB_OK;
+}
+
+int cvcb_time_stencil(cvcb_lattice *L, int kind, int precision, int link_recon, int nrhs,
+                      int reps, double *ms_per_launch) {
+  if (!L || !ms_per_launch) return CVCB_ERR_NULL;
+  CVCB_CUDA(cudaSetDevice(L->device));
+  return cvcb::time_stencil(L, kind, precision, link_recon, nrhs, reps, ms_per_launch);
+}
+
+int cvcb_solve(cvcb_lattice *L, double *const *x, const double *const *b, int nrhs,
+               const cvcb_solver_params *params, cvcb_solver_stats *stats) {
+  if (!L || !x || !b || !params || !stats) return CVCB_ERR_NULL;
+  for (int i = 0; i < nrhs; ++i)
+    if (!x[i] || !b[i]) return CVCB_ERR_NULL;
+  CVCB_CUDA(cudaSetDevice(L->device));
+  return cvcb::solve_batched(L, x, b, nrhs, params, stats);
+}
+
+}  // extern "C"

@@ -1,0 +1,265 @@
+/* cvcb.h -- C ABI of the B200 implementation of CVC's propagator-and-
+ * contraction path: the twisted-mass Wilson operator with boundary phases,
+ * the BiCGStab/CG propagator solvers with their reductions, and the
+ * conserved-vector-current contraction Pi_mu_nu(x).
+ *
+ * Conventions shared by every entry point
+ * ---------------------------------------
+ * - Field layouts are CVC's own (global.h:55-61 of the reference):
+ *     spinor field : 24 doubles per site, site ix at 24*ix, component
+ *                    2*(3*spin + colour) + re/im;
+ *     gauge field  : 72 doubles per site, link U_mu(ix) at 18*(4*ix + mu),
+ *                    3x3 complex row-major, WITHOUT the boundary phase;
+ *     Pi_mu_nu     : conn[2*(16*ix + 4*mu + nu) + re/im].
+ *   Sites are CVC lexicographic, ix = ((t*LX + x)*LY + y)*LZ + z, mu = 0..3
+ *   is t, x, y, z.  All extents must be even.
+ * - Pointers may be host memory or device memory of the lattice's GPU; the
+ *   library detects which and copies host data through its own staging.
+ * - Every call is asynchronous with respect to nothing: it returns after its
+ *   results are in the caller's buffers.  Calls on one cvcb_lattice must come
+ *   from one host thread at a time (the reference is single-threaded too).
+ * - Return values: >= 0 success (solvers: iteration count), otherwise one of
+ *   the CVCB_* codes below.  The library never calls exit().
+ */
+#ifndef CVCB_H
+#define CVCB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  -2 and -3 are the reference's own solver returns
+ * (invert_Qtm.c:112-113, 242-251); the others are new. */
+#define CVCB_OK 0
+#define CVCB_ERR_ARG (-1)
+#define CVCB_ERR_NULL (-2)
+#define CVCB_NO_CONVERGENCE (-3)
+#define CVCB_BREAKDOWN (-4)
+#define CVCB_ERR_STATE (-5)
+#define CVCB_ERR_NOMEM (-6)
+#define CVCB_ERR_CUDA (-7)
+#define CVCB_ERR_TIMEOUT (-8)
+
+typedef struct cvcb_lattice cvcb_lattice;
+
+/* Human-readable text of the last error on this host thread. */
+const char *cvcb_last_error(void);
+/* Library version string. */
+const char *cvcb_version(void);
+
+/* ---------------------------------------------------------------------
+ * Geometry and tables (host only; no GPU needed)
+ * ------------------------------------------------------------------- */
+
+/* All index tables of the reference's init_geometry()/geometry() for a
+ * single process (cvc_geometry.c:17-465): g_ipt as the (T+2)*LX*LY*LZ block
+ * (rows t = T, T+1 zero), g_iup/g_idn as 4*V, g_lexic2eo, g_eo2lexic,
+ * g_iseven, g_isevent, g_lexic2eot, g_eot2lexic as V each.  Bit-exact with
+ * the reference.  Any pointer may be NULL to skip that table. */
+int cvcb_geometry_tables(int T, int LX, int LY, int LZ, int *ipt, int *iup, int *idn,
+                         int *lexic2eo, int *eo2lexic, int *iseven, int *isevent,
+                         int *lexic2eot, int *eot2lexic);
+
+/* gamma_permutation[16][24] / gamma_sign[16][24] of init_gamma
+ * (cvc_utils.c:707-1520), bit-exact. */
+int cvcb_gamma_tables(int *perm, int *sign);
+
+/* co_phase_up[mu] = exp(i pi BCangle[mu] / L_mu) (cvc_geometry.c:452-459);
+ * ph[2*mu] = re, ph[2*mu+1] = im. */
+int cvcb_boundary_phases(int T, int LX, int LY, int LZ, const double bc_angle[4], double ph[8]);
+
+/* ---------------------------------------------------------------------
+ * Input generation (host only).  The reference has no generator for the
+ * benchmark's gauge recipe, so this one is new; it uses the reference's RNG.
+ * ------------------------------------------------------------------- */
+
+/* RANLUX double-precision generator, restated from ranlxd.c:493-600
+ * (rlxd_init(level, seed) followed by ranlxd(r, n)).  Bit-exact with the
+ * reference for the same level and seed. */
+int cvcb_ranlxd(int level, int seed, double *r, long n);
+
+/* Gauge field U = exp(i eps H) per link, H = sum_a w_a lambda_a / 2 with
+ * w_a standard normal from Box-Muller over ranlxd (as rangauss,
+ * cvc_utils.c:2734-2760) after rlxd_init(1, seed); links filled in site
+ * order, mu = 0..3, 8 normals per link.  U is then re-unitarised
+ * (Gram-Schmidt on rows 0,1, row 2 = conj(row0 x row1)) so det U = 1 to
+ * rounding.  Output in CVC layout, 72*V doubles. */
+int cvcb_gauge_random(double *gauge, int T, int LX, int LY, int LZ, double eps, int seed);
+
+/* ---------------------------------------------------------------------
+ * Lattice context: one per GPU and host thread.  Holds the geometry, the
+ * parameters (g_kappa, g_mu, BCangle), the gauge field in device layouts,
+ * and device work space.
+ * ------------------------------------------------------------------- */
+int cvcb_lattice_create(cvcb_lattice **lat, int T, int LX, int LY, int LZ, int device);
+int cvcb_lattice_destroy(cvcb_lattice *lat);
+
+/* g_kappa, g_mu (the bare twisted mass, Q_phi.c:25-36) and BCangle[4]
+ * (default_input_values.h:24-27: 1, 0, 0, 0). */
+int cvcb_set_params(cvcb_lattice *lat, double kappa, double mu, const double bc_angle[4]);
+
+/* Replaces g_gauge_field (72*V doubles, CVC layout, no phase).  The link
+ * phases are applied inside the library, as Q_phi.c:66 does per use. */
+int cvcb_upload_gauge(cvcb_lattice *lat, const double *gauge);
+
+/* Largest deviation from SU(3) of the uploaded links: max over links of
+ * max(|U U^dagger - 1|_max, |det U - 1|).  Compressed-link solvers are only
+ * used when this is small (see cvcb_solver_params.link_recon). */
+int cvcb_gauge_unitarity(cvcb_lattice *lat, double *dev);
+
+/* ---------------------------------------------------------------------
+ * Operators (reference: Q_phi.c).  xi and phi must not overlap.
+ * ------------------------------------------------------------------- */
+
+/* xi = Q phi, Q = 1/(2 kappa) + i mu g5 - 1/2 sum_mu [(1 - g_mu) U_mu(x)
+ * phi(x+mu) + (1 + g_mu) U_mu(x-mu)^dagger phi(x-mu)], links times
+ * co_phase_up.  Replaces void Q_phi_tbc(double *xi, double *phi),
+ * Q_phi.c:38-188 (Q_phi.h:11). */
+int cvcb_Q_phi_tbc(cvcb_lattice *lat, double *xi, const double *phi);
+
+/* xi = -kappa sum_mu [...] (hopping term only, hopping-parameter
+ * normalisation).  Replaces void Hopping(double *xi, double *phi),
+ * Q_phi.c:399-528 (Q_phi.h:12). */
+int cvcb_Hopping(cvcb_lattice *lat, double *xi, const double *phi);
+
+/* xi = g5 Q(mutm) phi.  Replaces void Qf5(double *xi, double *phi,
+ * double mutm), Q_phi.c:789-934 (Q_phi.h:27). */
+int cvcb_Qf5(cvcb_lattice *lat, double *xi, const double *phi, double mutm);
+
+/* xi = Q(mutm) phi.  Replaces void Q_phi(double *xi, double *phi,
+ * const double mutm), Q_phi.c:1092-1242 (Q_phi.h:29). */
+int cvcb_Q_phi(cvcb_lattice *lat, double *xi, const double *phi, double mutm);
+
+/* phi = g5 phi in place.  Replaces void g5_phi(double *phi),
+ * Q_phi.c:350-362 (Q_phi.h:51). */
+int cvcb_g5_phi(cvcb_lattice *lat, double *phi);
+
+/* phi = (1 - i sign 2 kappa mu g5) phi / (1 + (2 kappa mu)^2) on the first
+ * V sites.  Replaces void mul_one_pm_imu_inv(double *phi, double sign,
+ * int V), Q_phi.c:576-589 (Q_phi.h:14). */
+int cvcb_mul_one_pm_imu_inv(cvcb_lattice *lat, double *phi, double sign, int V);
+
+/* ---------------------------------------------------------------------
+ * Reductions (reference: invert_Qtm.c:28-84).  Deterministic: the same
+ * inputs give the same bits on every call.
+ * ------------------------------------------------------------------- */
+
+/* w = sum_x xi(x)^dagger phi(x) over the first V sites (w[0] = re,
+ * w[1] = im).  Replaces void spinor_scalar_product_co(complex *w,
+ * double *xi, double *phi, int V) (invert_Qtm.h:10). */
+int cvcb_spinor_scalar_product_co(cvcb_lattice *lat, double *w, const double *xi,
+                                  const double *phi, int V);
+/* r = Re sum_x xi(x)^dagger phi(x).  Replaces void
+ * spinor_scalar_product_re(double *r, double *xi, double *phi, int V)
+ * (invert_Qtm.h:9). */
+int cvcb_spinor_scalar_product_re(cvcb_lattice *lat, double *r, const double *xi,
+                                  const double *phi, int V);
+
+/* ---------------------------------------------------------------------
+ * FP64 solvers with the reference's algorithms and stopping rule:
+ * |r|^2 <= solver_precision * |phi|^2 (squared norms, invert_Qtm.c:201).
+ * xi holds the start guess on entry and the solution on exit.
+ * Returns the iteration count, CVCB_ERR_NULL or CVCB_NO_CONVERGENCE as the
+ * reference does.  true_res2 (may be NULL) receives |Q xi - phi|^2/|phi|^2.
+ * ------------------------------------------------------------------- */
+
+/* BiCGStab on Q.  Replaces int invert_Qtm(double *xi, double *phi,
+ * int kwork), invert_Qtm.c:86-270 (invert_Qtm.h:11); the work fields
+ * g_spinor_field[kwork..kwork+5] become device work space. */
+int cvcb_invert_Qtm(cvcb_lattice *lat, double *xi, const double *phi, double solver_precision,
+                    int niter_max, double *true_res2);
+
+/* BiCGStab on g5 Q(mu) g5 Q(-mu) = Q(-mu)^dagger Q(-mu) with right-hand
+ * side g5 phi, then xi = g5 Q(-mu) y.  Replaces int invert_Qtm_her(double
+ * *xi, double *phi, int kwork), invert_Qtm.c:276-478 (invert_Qtm.h:12). */
+int cvcb_invert_Qtm_her(cvcb_lattice *lat, double *xi, const double *phi,
+                        double solver_precision, int niter_max, double *true_res2);
+
+/* ---------------------------------------------------------------------
+ * Batched solver: even/odd preconditioned CG on the normal equations of the
+ * Schur complement, N right-hand sides per launch, optional reduced
+ * precision with FP64 reliable updates.  No counterpart in the reference
+ * (it reads propagators from files or calls tmLQCD, cvc_exact2_xspace.c:
+ * 401-547); it solves the same system Q x = b.
+ * ------------------------------------------------------------------- */
+#define CVCB_PREC_DOUBLE 0
+#define CVCB_PREC_SINGLE 1
+#define CVCB_PREC_HALF 2
+
+typedef struct {
+  int precision;     /* CVCB_PREC_*: arithmetic/storage of the inner iterations */
+  int link_recon;    /* 18 or 12 reals per link in the inner operator */
+  int block_rhs;     /* right-hand sides per launch (0 = autotuned) */
+  int block_threads; /* threads per block in the stencil (0 = autotuned) */
+  int max_iter;      /* per right-hand side */
+  int use_graph;     /* capture the inner iterations in a CUDA graph */
+  double tol;        /* target |b - Q x|_2 / |b|_2, checked in FP64 */
+  double delta;      /* reliable-update trigger: sloppy |r| fell by this factor */
+} cvcb_solver_params;
+
+typedef struct {
+  int iterations;        /* inner iterations, summed over right-hand sides */
+  int reliable_updates;  /* FP64 residual recomputations */
+  int restarts;          /* tightening restarts after the final FP64 check */
+  int converged;         /* right-hand sides that met tol */
+  double max_true_res;   /* max over rhs of |b - Q x| / |b| in FP64 */
+  double seconds;        /* device time of the solve */
+} cvcb_solver_stats;
+
+/* Fills the defaults: single precision, 12-real links, autotuned blocks,
+ * tol 1e-10, delta 0.1, max_iter 20000, graphs on. */
+void cvcb_solver_defaults(cvcb_solver_params *p);
+
+/* x[i], b[i] for i < nrhs: CVC-layout spinor fields (host or device).  x is
+ * output only (start guess zero). */
+int cvcb_solve(cvcb_lattice *lat, double *const *x, const double *const *b, int nrhs,
+               const cvcb_solver_params *params, cvcb_solver_stats *stats);
+
+/* Average duration of one stencil launch on device-resident fields, timed
+ * with CUDA events on the lattice's stream over `reps` back-to-back launches
+ * after one warm-up launch.  kind 0: the full-lattice FP64 kernel behind
+ * cvcb_Q_phi_tbc (one field, all V sites); kind 1: one half-lattice sweep of
+ * the batched solver's stencil (V/2 output sites) for nrhs right-hand sides
+ * in the given precision and link format, with the autotuned launch shape.
+ * Field contents are zero (timing does not depend on them). */
+int cvcb_time_stencil(cvcb_lattice *lat, int kind, int precision, int link_recon, int nrhs,
+                      int reps, double *ms_per_launch);
+
+/* Launch shape the autotuner chose for the batched stencil (sites and
+ * right-hand sides per thread block) for this lattice volume, precision,
+ * link format and batch size; CVCB_ERR_STATE before the first tuning. */
+int cvcb_tuned_shape(cvcb_lattice *lat, int precision, int link_recon, int nrhs,
+                     int *sites_per_block, int *rhs_per_block);
+
+/* ---------------------------------------------------------------------
+ * Contractions
+ * ------------------------------------------------------------------- */
+
+/* Conserved-vector-current two-point function Pi_mu_nu(x) for one source
+ * point, as cvc_exact2_xspace.c:577-861 computes it (including the -1/4
+ * normalisation at :861).  fields[0..59]: "up" propagators, 12 spin-colour
+ * columns (3*spin + colour) for each of the 5 source points y+mu (mu =
+ * 0..3) and y (index 4), at fields[12*mu + sc]; fields[60..119]: "dn"
+ * propagators in the same order.  source_site: lexicographic index of y.
+ * conn: 32*V doubles (output); contact: 8 doubles (output, the contact term
+ * printed at :697-716,837-855), may be NULL. */
+int cvcb_cvc_contract(cvcb_lattice *lat, const double *const *fields, int source_site,
+                      double *conn, double *contact);
+
+/* Ward-identity divergence sum_mu [Pi_mu_nu(x) - Pi_mu_nu(x - mu)]
+ * (cvc_exact2_xspace.c:928-1008); wi: 8*V doubles, wi[8*ix + 2*nu + re/im]. */
+int cvcb_cvc_ward(cvcb_lattice *lat, const double *conn, double *wi);
+
+/* Sequential source for the P -> gamma gamma three-point function
+ * (p2gg_xspace.c:525-539): source = exp(i (1 - 2 pos) 2 pi p.x / L)
+ * Gamma[gamma_id] prop(x) on timeslice t, zero elsewhere. */
+int cvcb_p2gg_seq_source(cvcb_lattice *lat, double *source, const double *prop, int timeslice,
+                         const int momentum[3], int gamma_id, int propagator_position);
+
+/* Plaquette <Re tr U_munu>/(18 V) and link sum (cvc_utils.c:384-436). */
+int cvcb_plaquette(cvcb_lattice *lat, double *plaq, double *linksum);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,139 @@
+"""FP64 BiCGStab solvers (invert_Qtm.c:86-478) and the batched mixed-
+precision solver against the oracle.
+
+Tolerances: the reference stops on the squared relative residual
+(solver_precision = 1e-20 for a true relative residual of 1e-10); two FP64
+solutions of the same system that both meet that bound agree to about
+cond(Q) * 1e-10, so solutions are compared at 1e-8 relative; the returned
+true residual must meet the bound itself."""
+import numpy as np
+import pytest
+
+from conftest import rel_err, seeded
+
+pytestmark = pytest.mark.gpu
+
+DIMS = (8, 4, 4, 4)
+KAPPA, MU = 0.15, 0.01 / 0.3
+
+
+@pytest.fixture(scope="module")
+def env(cb, oracle_mod):
+    lat = cb.Lattice(*DIMS, kappa=KAPPA, mu=MU)
+    g = cb.gauge_random(*DIMS, 0.3, 1234)
+    lat.upload_gauge(g)
+    orc = oracle_mod.Oracle(*DIMS, KAPPA, MU)
+    orc.set_gauge(g)
+    yield lat, orc, g
+    lat.close()
+
+
+def point_source(V, sc, site=0):
+    b = np.zeros(24 * V)
+    b[24 * site + 2 * sc] = 1.0
+    return b
+
+
+def test_invert_Qtm_her_point_source(env):
+    lat, orc, _ = env
+    V = lat.VOLUME
+    b = point_source(V, 0)
+    x = np.zeros(24 * V)
+    n, tr2 = lat.invert_Qtm_her(x, b, 1e-20, 1000, return_residual=True)
+    rc, xo, tro = orc.invert(b, 1e-20, 1000, her=True)
+    assert n > 0 and rc > 0
+    assert abs(n - rc) <= max(3, rc // 10)
+    assert tr2 < 1e-19
+    assert rel_err(x, xo) < 1e-8
+
+
+def test_invert_Qtm_breaks_down_on_point_source(env):
+    """<r2, r1> = 0 at the first step for a point source (the reference's
+    plain BiCGStab fails with NaN and returns -3)."""
+    lat, orc, _ = env
+    V = lat.VOLUME
+    b = point_source(V, 3)
+    x = np.zeros(24 * V)
+    assert lat.invert_Qtm(x, b, 1e-20, 50) == -3
+    rc, _, _ = orc.invert(b, 1e-20, 50, her=False)
+    assert rc == -3
+
+
+def test_invert_Qtm_random_source_subcritical(cb, oracle_mod):
+    lat = cb.Lattice(*DIMS, kappa=0.10, mu=0.02)
+    g = cb.gauge_random(*DIMS, 0.3, 99)
+    lat.upload_gauge(g)
+    orc = oracle_mod.Oracle(*DIMS, 0.10, 0.02)
+    orc.set_gauge(g)
+    b = seeded(5, 24 * lat.VOLUME)
+    x = np.zeros_like(b)
+    n, tr2 = lat.invert_Qtm(x, b, 1e-24, 1000, return_residual=True)
+    rc, xo, _ = orc.invert(b, 1e-24, 1000, her=False)
+    assert n > 0 and rc > 0 and abs(n - rc) <= 3
+    assert tr2 < 1e-23
+    assert rel_err(x, xo) < 1e-9
+    lat.close()
+
+
+def test_start_guess_already_solves(env):
+    """invert_Qtm.c:144-147: returns 0 and leaves xi untouched."""
+    lat, orc, _ = env
+    V = lat.VOLUME
+    x = seeded(8, 24 * V)
+    b = np.zeros(24 * V)
+    lat.Q_phi_tbc(b, x)
+    x0 = x.copy()
+    assert lat.invert_Qtm(x, b, 1e-10, 100) == 0
+    assert np.array_equal(x, x0)
+
+
+def test_null_field(cb, env):
+    lat, _, _ = env
+    b = np.zeros(24 * lat.VOLUME)
+    assert lat._lib.cvcb_invert_Qtm_her(lat._h, None, b.ctypes.data, 1e-20, 10, None) == -2
+
+
+@pytest.mark.parametrize("prec,recon", [(0, 18), (1, 12), (1, 18), (2, 12)],
+                         ids=["fp64", "fp32-12", "fp32-18", "fp16-12"])
+def test_batched_solver(cb, env, prec, recon):
+    lat, orc, _ = env
+    V = lat.VOLUME
+    bs = [point_source(V, sc) for sc in range(12)]
+    xs = [np.zeros(24 * V) for _ in range(12)]
+    p = cb.solver_defaults()
+    p.precision, p.link_recon, p.tol = prec, recon, 1e-10
+    st = lat.solve(xs, bs, p)
+    assert st.converged == 12
+    assert st.max_true_res <= 1e-10
+    # true residual recomputed independently by the full FP64 operator
+    for sc in (0, 5, 11):
+        r = np.zeros(24 * V)
+        lat.Q_phi_tbc(r, xs[sc])
+        assert np.linalg.norm(r - bs[sc]) / np.linalg.norm(bs[sc]) <= 1e-10
+    rc, xo, _ = orc.invert(bs[0], 1e-24, 2000, her=True)
+    assert rel_err(xs[0], xo) < 1e-8
+
+
+def test_batched_solver_device_pointers(cb, env):
+    torch = pytest.importorskip("torch")
+    lat, _, _ = env
+    V = lat.VOLUME
+    bs = [torch.from_numpy(seeded(20 + i, 24 * V)).cuda() for i in range(5)]
+    xs = [torch.zeros(24 * V, dtype=torch.float64, device="cuda") for _ in range(5)]
+    st = lat.solve(xs, bs)
+    torch.cuda.synchronize()
+    assert st.converged == 5 and st.max_true_res <= 1e-10
+    r = np.zeros(24 * V)
+    lat.Q_phi_tbc(r, xs[2].cpu().numpy())
+    b2 = bs[2].cpu().numpy()
+    assert np.linalg.norm(r - b2) / np.linalg.norm(b2) <= 1e-10
+
+
+def test_batched_solver_zero_rhs(cb, env):
+    lat, _, _ = env
+    V = lat.VOLUME
+    bs = [np.zeros(24 * V), point_source(V, 1)]
+    xs = [np.ones(24 * V), np.zeros(24 * V)]
+    st = lat.solve(xs, bs)
+    assert st.converged == 2
+    assert not np.any(xs[0])

@@ -1,0 +1,104 @@
+"""Host-side parts of the product that need no GPU: geometry tables, gamma
+tables, boundary phases, RANLUX, the gauge generator, propagator file
+names, and the C ABI's symbol table."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+FIX = np.load(os.path.join(HERE, "golden", "reference_fixtures.npz"))
+
+
+@pytest.mark.parametrize("dims", [(8, 4, 4, 4), (6, 4, 2, 4)])
+def test_geometry_bit_exact(cb, dims):
+    t = cb.geometry_tables(*dims)
+    tag = "x".join(map(str, dims))
+    for k, v in t.items():
+        assert np.array_equal(v, FIX[f"geom_{tag}_{k}"]), k
+
+
+def test_geometry_properties(cb):
+    T, LX, LY, LZ = 6, 4, 8, 2
+    t = cb.geometry_tables(T, LX, LY, LZ)
+    V = T * LX * LY * LZ
+    iup, idn = t["g_iup"].reshape(V, 4), t["g_idn"].reshape(V, 4)
+    for mu in range(4):
+        assert np.array_equal(idn[iup[:, mu], mu], np.arange(V))
+    assert sorted(t["g_eo2lexic"]) == list(range(V))
+    assert np.array_equal(t["g_lexic2eo"][t["g_eo2lexic"]], np.arange(V))
+
+
+def test_gamma_tables(cb):
+    perm, sign = cb.gamma_tables()
+    assert np.array_equal(perm, FIX["gamma_perm"])
+    assert np.array_equal(sign, FIX["gamma_sign"])
+
+
+@pytest.mark.parametrize("bc", [(1.0, 0.0, 0.0, 0.0), (1.0, 0.5, 0.0, 0.25)])
+def test_phases(cb, bc):
+    ph = cb.boundary_phases(8, 6, 4, 2, bc)
+    ref = FIX["phase_8x6x4x2_" + "_".join(str(b) for b in bc)]
+    assert np.array_equal(np.stack([ph.real, ph.imag], 1).ravel(), ref)
+
+
+@pytest.mark.parametrize("seed,level", [(1234, 1), (7, 2), (11, 1), (3, 1), (21, 1), (1, 1)])
+def test_ranlxd_bit_exact(cb, seed, level):
+    ref = FIX[f"ranlxd_{seed}_{level}"]
+    assert np.array_equal(cb.ranlxd(ref.size, seed, level), ref)
+
+
+def test_gauge_generator(cb):
+    g = cb.gauge_random(4, 2, 2, 4, 0.3, 1234)
+    u = (g[0::2] + 1j * g[1::2]).reshape(-1, 3, 3)
+    eye = np.eye(3)
+    assert np.max(np.abs(u @ np.conj(np.transpose(u, (0, 2, 1))) - eye)) < 1e-14
+    assert np.max(np.abs(np.linalg.det(u) - 1)) < 1e-14
+    assert np.array_equal(g, cb.gauge_random(4, 2, 2, 4, 0.3, 1234))
+    assert not np.array_equal(g, cb.gauge_random(4, 2, 2, 4, 0.3, 1235))
+    # small eps: close to the identity, with the first links drawn from
+    # ranlxd seed 1234 through Box-Muller (H traceless hermitian)
+    s = cb.gauge_random(2, 2, 2, 2, 1e-6, 1234)
+    us = (s[0::2] + 1j * s[1::2]).reshape(-1, 3, 3)
+    H = (us - eye) / 1e-6 / 1j
+    assert np.max(np.abs(H - np.conj(np.transpose(H, (0, 2, 1))))) < 1e-5
+    assert np.max(np.abs(np.trace(H, axis1=1, axis2=2))) < 1e-5
+    r = cb.ranlxd(8, 1234)
+    w0 = np.sqrt(-2 * np.log(r[0])) * np.cos(2 * np.pi * r[1])  # lambda_1 weight
+    assert abs(H[0, 0, 1].real - w0 / 2) < 1e-5
+
+
+def test_get_filename(cb):
+    from cvc_b200.files import get_filename
+    cases = [(0, 4, 7, 1), (0, 2, 11, -1), (0, 1, 0, 0), (2, 3, 5, 1), (3, 0, 9, -1), (4, 4, 2, 1)]
+    for (fmt, nu, sc, sign), want in zip(cases, FIX["filenames"]):
+        got = get_filename(nu, sc, sign, filename_prefix="source", filename_prefix2="dnprop",
+                           Nconf=17, format=fmt, source_location=37, T_global=8, LX_global=4,
+                           LY_global=4, LZ_global=4)
+        assert got == str(want)
+
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, "include", "cvcb.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cvcb_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(cb):
+    from cvc_b200 import _lib
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    declared = _declared_symbols()
+    assert len(declared) >= 30
+    for name in declared:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, name
+    assert set(_lib.SIGNATURES) == set(declared)
+
+
+def test_no_gpu_needed_for_host_api(cb):
+    # geometry and generators work without touching a device
+    assert cb.geometry_tables(2, 2, 2, 2)["g_iup"].size == 64
+    assert cb.last_error() is not None
