@@ -82,6 +82,8 @@ SIGNATURES = {
     "cvcb_solve": (_I, [_P, _P, _P, _I, ctypes.POINTER(SolverParams), ctypes.POINTER(SolverStats)]),
     "cvcb_time_stencil": (_I, [_P, _I, _I, _I, _I, _I, _DP]),
     "cvcb_tuned_shape": (_I, [_P, _I, _I, _I, _IP, _IP]),
+    "cvcb_profile": (_I, [_P, _I]),
+    "cvcb_counters": (_I, [_P, _P, _P, _P, _P]),
     "cvcb_cvc_contract": (_I, [_P, _P, _I, _P, _P]),
     "cvcb_cvc_ward": (_I, [_P, _P, _P]),
     "cvcb_p2gg_seq_source": (_I, [_P, _P, _P, _I, _P, _I, _I]),

@@ -351,11 +351,11 @@ int cvc_contract(cvcb_lattice *L, const double *const *fields, int src, double *
           }
         }
     k_cvc_z<<<blocks, 128, 0, L->stream>>>(static_cast<double2 *>(zb), P + 60 * fs, plan, g.V);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
     k_cvc_pi<<<blocks, 128, 0, L->stream>>>(static_cast<double *>(cb), P + 48 * fs,
                                             P + (size_t)nu * 12 * fs,
                                             static_cast<const double2 *>(zb), L->U64, g, nu);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
   }
   CVCB_TRY(conn_out(L, conn, static_cast<const double *>(cb), (size_t)g.V * 32));
 
@@ -424,7 +424,7 @@ int cvc_ward(cvcb_lattice *L, const double *conn, double *wi) {
                             L->stream));
   k_cvc_ward<<<(g.V + 127) / 128, 128, 0, L->stream>>>(static_cast<double *>(wb),
                                                         static_cast<const double *>(cb), g);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   CVCB_CUDA(cudaMemcpyAsync(wi, wb, (size_t)g.V * 8 * sizeof(double), cudaMemcpyDefault,
                             L->stream));
   CVCB_CUDA(cudaStreamSynchronize(L->stream));
@@ -462,7 +462,7 @@ int p2gg_seq_source(cvcb_lattice *L, double *source, const double *prop, int t, 
   const double sgn2pi = (1. - 2. * pos) * 2. * M_PI;
   k_seq_source<<<(g.V + 127) / 128, 128, 0, L->stream>>>(dsrc, dprop, g, t, mom[0], mom[1], mom[2],
                                                           sgn2pi, gt);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   if (host_out)
     CVCB_CUDA(cudaMemcpyAsync(source, dsrc, bytes, cudaMemcpyDeviceToHost, L->stream));
   CVCB_CUDA(cudaStreamSynchronize(L->stream));
@@ -491,7 +491,7 @@ int plaquette(cvcb_lattice *L, double *plaq, double *linksum) {
                             cudaMemcpyHostToDevice, L->stream));
   k_gauge_raw_eo<<<(g.V + 127) / 128, 128, 0, L->stream>>>(static_cast<double2 *>(eo),
                                                             static_cast<const double2 *>(raw), g);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   CVCB_TRY(launch_reduce<1>(L, PlaqF{static_cast<const double2 *>(eo), g},
                             StorePlaq{L->red_result}, (size_t)g.V));
   CVCB_TRY(launch_reduce<2>(L, LinkSumF{static_cast<const double2 *>(raw)},

@@ -48,6 +48,13 @@ const char *last_error();
     }                                                                                \
   } while (0)
 
+// After a kernel launch: count it and surface launch errors.
+#define CVCB_LAUNCHED(Lp)                \
+  do {                                   \
+    ++(Lp)->nlaunch;                     \
+    CVCB_CUDA(cudaGetLastError());       \
+  } while (0)
+
 #define CVCB_TRY(expr)             \
   do {                             \
     int r_ = (expr);               \
@@ -160,6 +167,13 @@ struct cvcb_lattice {
 
   // named device buffers, grown on demand
   std::vector<cvcb::Buffer> bufs;
+
+  // instrumentation: kernels launched by this context (graph launches count
+  // their kernel nodes), and CUDA-event timing of the solver's stencil
+  long long nlaunch = 0;
+  bool prof = false;
+  long long prof_launches = 0;
+  double prof_ms = 0.0, prof_bytes = 0.0;
 };
 
 namespace cvcb {

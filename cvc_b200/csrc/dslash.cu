@@ -130,7 +130,7 @@ int launch_tm_full(cvcb_lattice *L, double2 *out, const double2 *in, double a, d
     g_tm_variant = bestv;
   }
   launch_by_variant(g_tm_variant, L, out, in, a, b, c, g5out, done);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   return CVCB_OK;
 }
 
@@ -148,7 +148,7 @@ __global__ void k_g5(double2 *f, Geom g, int nsites_lex) {
 
 int launch_g5(cvcb_lattice *L, double2 *f, int nsites) {
   k_g5<<<(nsites + 127) / 128, 128, 0, L->stream>>>(f, L->g, nsites);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   return CVCB_OK;
 }
 
@@ -172,7 +172,7 @@ int launch_one_pm_imu_inv(cvcb_lattice *L, double2 *f, double sign, int nsites) 
   const double m = 2.0 * L->kappa * L->mu;
   k_one_pm_imu_inv<<<(nsites + 127) / 128, 128, 0, L->stream>>>(f, L->g, nsites, -sign * m,
                                                                   1.0 / (1.0 + m * m));
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   return CVCB_OK;
 }
 

@@ -9,10 +9,9 @@
 //   out_p = D2 aux_p + D1 ( c [g5] H_pq ([g5] in_q) )
 // with D1, D2 site-diagonal operators alpha + i beta g5.
 //
-// Thread mapping: x = site within the output parity, y = right-hand side.
-// The y-threads of one block handle different right-hand sides of the same
-// sites, so each link is fetched from HBM once and served from L1 to the
-// others ("multi-RHS": link traffic / N).
+// Multi-RHS: the threads that handle the same sites for different
+// right-hand sides share each link load (registers within a thread, L1/L2
+// across threads), so link traffic per right-hand side falls as 1/N.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -238,72 +237,103 @@ struct HopArgs {
   double c;         // hop coefficient
 };
 
-// Grid: blockIdx.x = group of right-hand sides (fastest), blockIdx.y (and a
-// stride loop) = block of sites.  Blocks that run back to back therefore
-// share their sites, and a link fetched for one group of right-hand sides
-// is still in L2 (or L1) for the next.
+// Thread mapping: each thread handles one output site for NR right-hand
+// sides; blockDim.y groups of NR share the block.  The link of every
+// direction is loaded (and, for 12-real storage, rebuilt and multiplied by
+// its phase) once per thread and applied to all NR spinors from registers.
+// Grid: blockIdx.x = block of rhs groups (fastest), blockIdx.y (and a stride
+// loop) = block of sites, so consecutive blocks share their sites' links in
+// L2.
 constexpr int kHopMaxThreads = 256;
 
-template <class SF, class LF, bool G5IN, bool G5HOP, bool AUX>
+template <typename R, class LF>
+__device__ __forceinline__ Link<R> phased_link(const LF &lk, int mu, int j) {
+  Link<R> W = lk.load(mu, j);
+  if (!LF::kPhased) {
+    const Cx<R> ph = cx((R)lk.ph[mu].x, (R)lk.ph[mu].y);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) W.m[a][b] = cmul(W.m[a][b], ph);
+  }
+  return W;
+}
+
+template <class SF, class LF, int NR, bool G5IN, bool G5HOP, bool AUX>
 __global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop(HopArgs<SF, LF> A) {
   using R = typename SF::R;
-  const int r = blockIdx.x * blockDim.y + threadIdx.y;
+  const int r0 = (blockIdx.x * blockDim.y + threadIdx.y) * NR;
   const Geom &g = A.eg.g;
-  if (r >= A.nrhs) return;
-  if (A.done && A.done[r]) return;
-  for (int sb = blockIdx.y; sb * (int)blockDim.x < g.Vh; sb += gridDim.y) {
-  const int i = sb * blockDim.x + threadIdx.x;
-  if (i >= g.Vh) return;
+  if (r0 >= A.nrhs) return;
+  bool act[NR];
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    act[k] = r0 + k < A.nrhs && !(A.done && A.done[r0 + k]);
+    any = any || act[k];
+  }
+  if (!any) return;
   const int p = A.eg.p;
-  const SiteCoord cd = site_coord(g, p, i);
-  const int self = p * g.Vh + i;  // link index of this site (links are full-lattice)
   const int qoff = (1 - p) * g.Vh;
+  for (int sb = blockIdx.y; sb * (int)blockDim.x < g.Vh; sb += gridDim.y) {
+    const int i = sb * blockDim.x + threadIdx.x;
+    if (i >= g.Vh) return;
+    const SiteCoord cd = site_coord(g, p, i);
+    const int self = p * g.Vh + i;
 
-  Spinor<R> acc;
+    Spinor<R> acc[NR];
 #pragma unroll
-  for (int s = 0; s < 4; ++s)
+    for (int k = 0; k < NR; ++k)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) acc.c[s][c] = cx((R)0, (R)0);
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[k].c[s][c] = cx((R)0, (R)0);
 
 #pragma unroll
-  for (int mu = 0; mu < 4; ++mu) {
-    {  // backward
-      const int j = nb_lex(g, cd, mu, -1) >> 1;
-      Spinor<R> f = A.in.load(r, j);
-      if (G5IN) g5_inplace(f);
-      const HalfSpinor<R> h = project(mu, +1, f);
-      const Link<R> W = A.links.load(mu, qoff + j);
-      HalfSpinor<R> u = link_dag_mul(W, h);
-      if (!LF::kPhased) u = cscale(u, cx((R)A.links.ph[mu].x, (R)-A.links.ph[mu].y));
-      accum_recon(mu, +1, acc, u);
+    for (int mu = 0; mu < 4; ++mu) {
+      {  // backward: (1 + g_mu) U_mu(x-mu)^+ in(x-mu)
+        const int j = nb_lex(g, cd, mu, -1) >> 1;
+        const Link<R> W = phased_link<R>(A.links, mu, qoff + j);
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+          if (!act[k]) continue;
+          Spinor<R> f = A.in.load(r0 + k, j);
+          if (G5IN) g5_inplace(f);
+          accum_recon(mu, +1, acc[k], link_dag_mul(W, project(mu, +1, f)));
+        }
+      }
+      {  // forward: (1 - g_mu) U_mu(x) in(x+mu)
+        const int j = nb_lex(g, cd, mu, +1) >> 1;
+        const Link<R> W = phased_link<R>(A.links, mu, self);
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+          if (!act[k]) continue;
+          Spinor<R> f = A.in.load(r0 + k, j);
+          if (G5IN) g5_inplace(f);
+          accum_recon(mu, -1, acc[k], link_mul(W, project(mu, -1, f)));
+        }
+      }
     }
-    {  // forward
-      const int j = nb_lex(g, cd, mu, +1) >> 1;
-      Spinor<R> f = A.in.load(r, j);
-      if (G5IN) g5_inplace(f);
-      const HalfSpinor<R> h = project(mu, -1, f);
-      const Link<R> W = A.links.load(mu, self);
-      HalfSpinor<R> u = link_mul(W, h);
-      if (!LF::kPhased) u = cscale(u, cx((R)A.links.ph[mu].x, (R)A.links.ph[mu].y));
-      accum_recon(mu, -1, acc, u);
+    const R c = (R)A.c;
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      if (!act[k]) continue;
+      if (G5HOP) g5_inplace(acc[k]);
+      Spinor<R> o;
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) o.c[s][q] = c * acc[k].c[s][q];
+      o = diag_op((R)A.d1a, (R)A.d1b, o);
+      if (AUX) {
+        const Spinor<R> x = diag_op((R)A.d2a, (R)A.d2b, A.aux.load(r0 + k, i));
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+          for (int q = 0; q < 3; ++q) o.c[s][q] = o.c[s][q] + x.c[s][q];
+      }
+      A.out.store(r0 + k, i, o);
     }
-  }
-  if (G5HOP) g5_inplace(acc);
-  Spinor<R> o;
-  const R c = (R)A.c;
-#pragma unroll
-  for (int s = 0; s < 4; ++s)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o.c[s][k] = c * acc.c[s][k];
-  o = diag_op((R)A.d1a, (R)A.d1b, o);
-  if (AUX) {
-    const Spinor<R> x = diag_op((R)A.d2a, (R)A.d2b, A.aux.load(r, i));
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) o.c[s][k] = o.c[s][k] + x.c[s][k];
-  }
-  A.out.store(r, i, o);
   }
 }
 

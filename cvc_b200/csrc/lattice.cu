@@ -87,7 +87,7 @@ int spinor_in(cvcb_lattice *L, double2 *dst, const double *src, int nsites) {
     dsrc = static_cast<const double2 *>(st);
   }
   k_spinor_aos_to_eo<<<(g.V + 127) / 128, 128, 0, L->stream>>>(dst, dsrc, g, nsites);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   return CVCB_OK;
 }
 
@@ -96,14 +96,14 @@ int spinor_out(cvcb_lattice *L, double *dst, const double2 *src, int nsites) {
   if (is_device_ptr(dst)) {
     k_spinor_eo_to_aos<<<(g.V + 127) / 128, 128, 0, L->stream>>>(
         reinterpret_cast<double2 *>(dst), src, g, nsites);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
     return CVCB_OK;
   }
   void *st;
   CVCB_TRY(ensure_buffer(L, SLOT_STAGE_B, (size_t)g.V * 24 * sizeof(double), &st));
   k_spinor_eo_to_aos<<<(g.V + 127) / 128, 128, 0, L->stream>>>(static_cast<double2 *>(st), src,
                                                                   g, nsites);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   CVCB_CUDA(cudaMemcpyAsync(dst, st, (size_t)nsites * 24 * sizeof(double),
                             cudaMemcpyDeviceToHost, L->stream));
   return CVCB_OK;
@@ -167,7 +167,7 @@ static int build_gauge_forms(cvcb_lattice *L) {
   k_gauge_forms<<<(g.V + 127) / 128, 128, 0, L->stream>>>(
       static_cast<const double2 *>(raw), g, make_double4(ph[0], ph[1], ph[2], ph[3]),
       make_double4(ph[4], ph[5], ph[6], ph[7]), L->U64, L->U32c, L->U32f, L->U16c);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   CVCB_CUDA(cudaStreamSynchronize(L->stream));
   return CVCB_OK;
 }

@@ -90,7 +90,7 @@ template <int NOUT, class F, class E>
 int launch_reduce(cvcb_lattice *L, F f, E e, size_t n, const int *skip = nullptr) {
   const int blocks = red_blocks(n);
   k_reduce<NOUT><<<blocks, kRedThreads, 0, L->stream>>>(f, e, n, L->partials, L->red_counter, skip);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   return CVCB_OK;
 }
 

@@ -240,7 +240,7 @@ int invert_bicgstab(cvcb_lattice *L, bool her, double *xi, const double *phi, do
   // p = rhs - A x ; norm = <p,p>
   CVCB_TRY(apply_op(L, her, p, x, aux, nullptr));
   k_sub<<<eb, 256, 0, L->stream>>>(p, rhs, p, n);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   CVCB_TRY(launch_reduce<1>(L, RedNorm{p}, EpiStart{S}, n));
   SolverScalars hs;
   CVCB_CUDA(cudaMemcpyAsync(&hs, S, sizeof hs, cudaMemcpyDeviceToHost, L->stream));
@@ -264,13 +264,13 @@ int invert_bicgstab(cvcb_lattice *L, bool her, double *xi, const double *phi, do
     for (int it = 0; it < todo; ++it) {
       CVCB_TRY(launch_reduce<4>(L, RedRhoW{r2, r1, p2}, EpiAlpha{S}, n, done));
       k_s_update<<<eb, 256, 0, L->stream>>>(s, r1, p2, S, n);
-      CVCB_CUDA(cudaGetLastError());
+      CVCB_LAUNCHED(L);
       CVCB_TRY(apply_op(L, her, t, s, aux, done));
       CVCB_TRY(launch_reduce<3>(L, RedOmega{t, s}, EpiOmega{S}, n, done));
       CVCB_TRY(launch_reduce<1>(L, RedR1{r1, s, t, S}, EpiNorm{S}, n, done));
       CVCB_TRY(launch_reduce<2>(L, RedXBeta{x, s, p, r2, r1, S}, EpiBeta{S}, n, done));
       k_p_update<<<eb, 256, 0, L->stream>>>(p, r1, p2, S, n);
-      CVCB_CUDA(cudaGetLastError());
+      CVCB_LAUNCHED(L);
       CVCB_TRY(apply_op(L, her, p2, p, aux, done));
     }
     launched += todo;
@@ -297,7 +297,7 @@ int invert_bicgstab(cvcb_lattice *L, bool her, double *xi, const double *phi, do
     // true residual |Q x - phi|^2 / |phi|^2 (invert_Qtm.c:257-267 / :466-475)
     CVCB_TRY(launch_tm_full(L, t, x, 0.5 / L->kappa, L->mu, -0.5, false, nullptr));
     k_sub<<<eb, 256, 0, L->stream>>>(t, t, phid, n);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
     double r2n;
     CVCB_TRY(dot_re(L, t, t, n, &r2n));
     *true_res2 = r2n / hs.normb;

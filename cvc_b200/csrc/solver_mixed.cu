@@ -19,10 +19,13 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <numeric>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "cvcb_internal.h"
@@ -279,7 +282,7 @@ struct RedResid {
 // The solver object for one batch
 // ---------------------------------------------------------------------------
 struct LaunchShape {
-  int bx = 64, by = 1;
+  int bx = 64, by = 1, nr = 1;  // sites per block, rhs groups per block, rhs per thread
 };
 
 // Autotuner results, per process: (V, precision, recon, n) -> launch shape,
@@ -288,6 +291,19 @@ std::map<std::tuple<int, int, int, int>, LaunchShape> g_tuned_shape;
 std::map<std::tuple<int, int, int, int>, int> g_tuned_batch;
 
 namespace {
+
+// Bytes of one stored spinor / link, for the algorithmic traffic model.
+template <class LF>
+constexpr double link_bytes();
+template <> constexpr double link_bytes<L64>() { return 144; }
+template <> constexpr double link_bytes<L32f>() { return 72; }
+template <> constexpr double link_bytes<L32c>() { return 48; }
+template <> constexpr double link_bytes<L16c>() { return 24; }
+template <class SF>
+constexpr double spinor_bytes();
+template <> constexpr double spinor_bytes<F64Acc>() { return 192; }
+template <> constexpr double spinor_bytes<F32Acc>() { return 96; }
+template <> constexpr double spinor_bytes<F16Acc>() { return 52; }  // 48 + float norm
 
 int red_blocks_sites(int n) {
   int b = (n + kRedThreads * 2 - 1) / (kRedThreads * 2);
@@ -313,6 +329,15 @@ struct Batch {
   LF links;
   L64 links64;
   double mu, kap;
+  // stencil timing (instrumentation): events recorded around the sloppy
+  // stencil launches of one iteration per chunk
+  bool prof_rec = false;
+  bool capturing = false;
+  struct Rec {
+    cudaEvent_t a, b;
+    double bytes_per_rhs, link_bytes;
+  };
+  std::vector<Rec> recs;
 
   F64Acc f64(double2 *base, int parity) const {
     return F64Acc{base + (size_t)parity * g.Vh, (size_t)g.V, (size_t)12 * g.V};
@@ -323,14 +348,35 @@ struct Batch {
   int hop(AF out, AF in, AF aux, LL lk, int parity, const int *done, double d1a, double d1b,
           double d2a, double d2b, double c) {
     HopArgs<AF, LL> a{out, in, aux, lk, EoGeom{g, parity}, n, done, d1a, d1b, d2a, d2b, c};
-    // FP64 sweeps (reliable updates) always use a fixed small shape
-    const LaunchShape sh = sizeof(typename AF::R) == 8 && sizeof(typename SF::R) != 8
-                               ? LaunchShape{64, 1} : shape;
-    const int by = std::min(sh.by, n);
+    // FP64 sweeps of a reduced-precision solve (reliable updates) use a
+    // fixed shape; FP64 kernels keep one rhs per thread (register budget).
+    LaunchShape sh = sizeof(typename AF::R) == 8 && sizeof(typename SF::R) != 8
+                         ? LaunchShape{64, 1, 1} : shape;
+    if (sizeof(typename AF::R) == 8) sh.nr = 1;
+    const int groups = (n + sh.nr - 1) / sh.nr;
+    const int by = std::min(sh.by, groups);
     const int site_blocks = (g.Vh + sh.bx - 1) / sh.bx;
-    dim3 block(sh.bx, by), grid((n + by - 1) / by, std::min(site_blocks, 65535));
-    k_eo_hop<AF, LL, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
-    CVCB_CUDA(cudaGetLastError());
+    dim3 block(sh.bx, by), grid((groups + by - 1) / by, std::min(site_blocks, 65535));
+    Rec rec{};
+    const bool rec_this = prof_rec && std::is_same<AF, SF>::value;
+    if (rec_this) {
+      CVCB_CUDA(cudaEventCreate(&rec.a));
+      CVCB_CUDA(cudaEventCreate(&rec.b));
+      CVCB_CUDA(cudaEventRecordWithFlags(rec.a, L->stream, capturing ? cudaEventRecordExternal : 0));
+    }
+    switch (sh.nr) {
+      case 2: k_eo_hop<AF, LL, 2, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
+      case 3: k_eo_hop<AF, LL, 3, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
+      case 4: k_eo_hop<AF, LL, 4, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
+      default: k_eo_hop<AF, LL, 1, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
+    }
+    CVCB_LAUNCHED(L);
+    if (rec_this) {
+      CVCB_CUDA(cudaEventRecordWithFlags(rec.b, L->stream, capturing ? cudaEventRecordExternal : 0));
+      rec.bytes_per_rhs = (double)g.Vh * spinor_bytes<AF>() * (AUX ? 3 : 2);
+      rec.link_bytes = 4.0 * g.V * link_bytes<LL>();
+      recs.push_back(rec);
+    }
     return CVCB_OK;
   }
 
@@ -363,13 +409,13 @@ struct Batch {
     dim3 rg(red_blocks_sites(g.Vh), n);
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedPAp<SF>{p, Ap}, EpiAlphaB{S}, g.Vh, br,
                                                     S.done);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedUpdate<SF, XF>{p, Ap, rs, xs, S},
                                                     EpiBetaB{S}, g.Vh, br, S.done);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
     dim3 eg((g.Vh + 127) / 128, n);
     k_p_upd<<<eg, 128, 0, L->stream>>>(p, rs, S, g.Vh, n);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
     return CVCB_OK;
   }
 
@@ -397,17 +443,17 @@ struct Batch {
     dim3 eg((g.Vh + 127) / 128, n);
     if (absorb) {
       k_absorb<<<eg, 128, 0, L->stream>>>(f64(x64, 1), xs, ru_skip, g.Vh, n);
-      CVCB_CUDA(cudaGetLastError());
+      CVCB_LAUNCHED(L);
     }
     CVCB_TRY(schur64(y64, x64, mu, ru_skip));
     dim3 rg(red_blocks_sites(g.Vh), n);
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedRhat{f64(bh64, 1), f64(y64, 1)},
                                                     EpiStore{S.rhat2}, g.Vh, br, ru_skip);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
     CVCB_TRY(schur64_dag(rn64, y64, ru_skip));
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedToSloppy<SF>{f64(rn64, 1), rs}, EpiRR{S},
                                                     g.Vh, br, ru_skip);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
     return CVCB_OK;
   }
 };
@@ -565,15 +611,32 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon) {
     B.shape = it->second;
     return CVCB_OK;
   }
+  // CVCB_SHAPE="sites,rows,rhs_per_thread" pins the shape (reproducible runs,
+  // profiling); otherwise every admissible shape is timed.
+  if (const char *env = getenv("CVCB_SHAPE")) {
+    LaunchShape f;
+    if (sscanf(env, "%d,%d,%d", &f.bx, &f.by, &f.nr) == 3 && f.bx > 0 && f.by > 0 && f.nr >= 1 &&
+        f.nr <= 4 && f.bx * f.by <= kHopMaxThreads) {
+      if (sizeof(typename SF::R) == 8) f.nr = 1;
+      B.shape = f;
+      g_tuned_shape[key] = f;
+      return CVCB_OK;
+    }
+  }
   LaunchShape best;
   float best_ms = 1e30f;
   const int bxs[] = {32, 64, 128, 256};
-  const int bys[] = {1, 2, 4, 8, 12};
-  for (int bx : bxs)
+  const int bys[] = {1, 2, 4};
+  const int nrs[] = {1, 2, 3, 4};
+  const bool fp64 = sizeof(typename SF::R) == 8;
+  for (int nr : nrs)
+    for (int bx : bxs)
     for (int by : bys) {
-      if (by > B.n || bx * by > kHopMaxThreads || bx * by < 32) continue;
+      if (fp64 && nr > 1) continue;
+      if (nr > B.n || by * nr > B.n || bx * by > kHopMaxThreads || bx * by < 32) continue;
       B.shape.bx = bx;
       B.shape.by = by;
+      B.shape.nr = nr;
       float ms;
       if (time_ms(L, [&] { return B.normal_op_sloppy(B.Ap, B.p, nullptr); }, 3, &ms) != CVCB_OK) {
         cudaGetLastError();
@@ -608,7 +671,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   double *bnorm2 = B.S.rn2;  // temporary use
   k_reduce_rhs<<<rgf, kRedThreads, 0, L->stream>>>(RedNorm64{B.f64full(B.b64)},
                                                    EpiStore{bnorm2}, g.V, B.br, nullptr);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   std::vector<double> hb2(n);
   CVCB_CUDA(cudaMemcpyAsync(hb2.data(), bnorm2, n * sizeof(double), cudaMemcpyDeviceToHost,
                             L->stream));
@@ -616,7 +679,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   double ia, ib;
   B.ainv(B.mu, ia, ib);
   k_diag64<<<eg, 128, 0, L->stream>>>(B.f64(B.t64, 0), B.f64(B.b64, 0), ia, ib, g.Vh, n);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   CVCB_TRY((B.template hop<F64Acc, L64, false, false, true>(B.f64(B.bh64, 1), B.f64(B.t64, 0),
                                                             B.f64(B.b64, 1), B.links64, 1,
                                                             nullptr, 1, 0, 1, 0, 0.5)));
@@ -626,7 +689,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   // x_s = 0 (all-zero bits are 0.0), p = r_s
   CVCB_CUDA(cudaMemsetAsync(B.xs_mem, 0, B.xs_bytes, L->stream));
   k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, nullptr, g.Vh, n);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   std::vector<double> rr(n), rr_max(n), rhat2(n), ratio2(n), target2(n);
   std::vector<int> done(n, 0), iters(n, 0), since(n, 0), skip(n, 0);
   CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
@@ -647,17 +710,45 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   // capture a chunk of iterations in a CUDA graph
   const int chunk = 10;
   cudaGraphExec_t gexec = nullptr;
+  long long graph_nodes = 0;
   if (P->use_graph) {
     cudaGraph_t graph;
+    const long long before = L->nlaunch;
     CVCB_CUDA(cudaStreamBeginCapture(L->stream, cudaStreamCaptureModeThreadLocal));
+    B.capturing = true;
     int rc = CVCB_OK;
-    for (int k = 0; k < chunk && rc == CVCB_OK; ++k) rc = B.iteration();
+    for (int k = 0; k < chunk && rc == CVCB_OK; ++k) {
+      B.prof_rec = L->prof && k == 0;
+      rc = B.iteration();
+    }
+    B.prof_rec = false;
+    B.capturing = false;
     cudaError_t ec = cudaStreamEndCapture(L->stream, &graph);
     if (rc != CVCB_OK) return rc;
     CVCB_CUDA(ec);
     CVCB_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
     cudaGraphDestroy(graph);
+    graph_nodes = L->nlaunch - before;  // kernels per graph launch
+    L->nlaunch = before;
   }
+  auto harvest = [&](int active) -> int {
+    // per-launch device time of the recorded stencil launches (instrumentation)
+    for (auto &r : B.recs) {
+      float ms;
+      CVCB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+      L->prof_ms += ms;
+      L->prof_launches += 1;
+      L->prof_bytes += r.bytes_per_rhs * active + r.link_bytes;
+    }
+    if (!gexec) {
+      for (auto &r : B.recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+      }
+      B.recs.clear();
+    }
+    return CVCB_OK;
+  };
 
   const double delta2 = P->delta * P->delta;
   int total_iter = 0, nru = 0;
@@ -668,6 +759,8 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     for (int i = 0; i < n; ++i) all = all && done[i];
     if (all) break;
     if (total_iter >= P->max_iter) break;
+    int active = 0;
+    for (int i = 0; i < n; ++i) active += !done[i];
     if (gexec) {
       cudaError_t e = cudaGraphLaunch(gexec, L->stream);
       if (e != cudaSuccess) {
@@ -675,15 +768,20 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
         rc = CVCB_ERR_CUDA;
         break;
       }
+      L->nlaunch += graph_nodes;
     } else {
-      for (int k = 0; k < chunk; ++k)
+      for (int k = 0; k < chunk; ++k) {
+        B.prof_rec = L->prof && k == 0;
         if ((rc = B.iteration()) != CVCB_OK) break;
+      }
+      B.prof_rec = false;
       if (rc != CVCB_OK) break;
     }
     total_iter += chunk;
     CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost,
                               L->stream));
     CVCB_CUDA(cudaStreamSynchronize(L->stream));
+    if (L->prof) CVCB_TRY(harvest(active));
     bool any = false;
     for (int i = 0; i < n; ++i) {
       skip[i] = 1;
@@ -704,7 +802,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     CVCB_TRY(B.reliable_update(true));
     // restart the search direction of updated rhs from the true residual
     k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.ru_skip, g.Vh, n);
-    CVCB_CUDA(cudaGetLastError());
+    CVCB_LAUNCHED(L);
     ++nru;
     CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost,
                               L->stream));
@@ -722,6 +820,11 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
                               L->stream));
   }
   if (gexec) cudaGraphExecDestroy(gexec);
+  for (auto &r : B.recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  B.recs.clear();
   if (rc != CVCB_OK) return rc;
 
   // x_e = A^-1 (b_e + 1/2 H_eo x_o)
@@ -737,7 +840,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   }
   k_reduce_rhs<<<rgf, kRedThreads, 0, L->stream>>>(
       RedResid{B.f64full(B.t64), B.f64full(B.b64)}, EpiStore{B.S.rhat2}, g.V, B.br, nullptr);
-  CVCB_CUDA(cudaGetLastError());
+  CVCB_LAUNCHED(L);
   CVCB_CUDA(cudaMemcpyAsync(rhat2.data(), B.S.rhat2, n * sizeof(double), cudaMemcpyDeviceToHost,
                             L->stream));
   for (int i = 0; i < n; ++i) CVCB_TRY(spinor_out(L, x[i], B.x64 + i * fs, g.V));
@@ -880,16 +983,38 @@ void cvcb_solver_defaults(cvcb_solver_params *p) {
   p->delta = 0.1;
 }
 
+int cvcb_profile(cvcb_lattice *L, int enable) {
+  if (!L) return CVCB_ERR_NULL;
+  L->prof = enable != 0;
+  if (enable) {
+    L->prof_launches = 0;
+    L->prof_ms = 0.0;
+    L->prof_bytes = 0.0;
+  }
+  return CVCB_OK;
+}
+
+int cvcb_counters(cvcb_lattice *L, long long *kernel_launches, long long *stencil_launches_timed,
+                  double *stencil_ms, double *stencil_bytes) {
+  if (!L) return CVCB_ERR_NULL;
+  if (kernel_launches) *kernel_launches = L->nlaunch;
+  if (stencil_launches_timed) *stencil_launches_timed = L->prof_launches;
+  if (stencil_ms) *stencil_ms = L->prof_ms;
+  if (stencil_bytes) *stencil_bytes = L->prof_bytes;
+  return CVCB_OK;
+}
+
 int cvcb_tuned_shape(cvcb_lattice *L, int precision, int link_recon, int nrhs, int *sites_per_block,
                      int *rhs_per_block) {
   if (!L || !sites_per_block || !rhs_per_block) return CVCB_ERR_NULL;
+  // rhs_per_block = rhs groups per block x rhs per thread
   auto it = cvcb::g_tuned_shape.find(std::make_tuple(L->g.V, precision, link_recon, nrhs));
   if (it == cvcb::g_tuned_shape.end()) {
     cvcb::set_error("no tuned shape for this configuration yet");
     return CVCB_ERR_STATE;
   }
   *sites_per_block = it->second.bx;
-  *rhs_per_block = it->second.by;
+  *rhs_per_block = it->second.by * 100 + it->second.nr;
   return CVCB_OK;
 }
 

@@ -225,11 +225,24 @@ int cvcb_solve(cvcb_lattice *lat, double *const *x, const double *const *b, int 
 int cvcb_time_stencil(cvcb_lattice *lat, int kind, int precision, int link_recon, int nrhs,
                       int reps, double *ms_per_launch);
 
-/* Launch shape the autotuner chose for the batched stencil (sites and
- * right-hand sides per thread block) for this lattice volume, precision,
- * link format and batch size; CVCB_ERR_STATE before the first tuning. */
+/* Launch shape the autotuner chose for the batched stencil for this lattice
+ * volume, precision, link format and batch size: sites per thread block, and
+ * rhs_per_block = 100 * (thread rows per block) + (right-hand sides per
+ * thread); CVCB_ERR_STATE before the first tuning. */
 int cvcb_tuned_shape(cvcb_lattice *lat, int precision, int link_recon, int nrhs,
                      int *sites_per_block, int *rhs_per_block);
+
+/* Instrumentation.  cvcb_profile(lat, 1) resets and starts timing the
+ * batched solver's stencil: inside cvcb_solve, the stencil launches of one
+ * iteration per chunk of iterations are bracketed by CUDA events on the
+ * solver's stream (also inside its CUDA graph), and their device time and
+ * algorithmic bytes (inputs, outputs and links read once; see
+ * cvcb_time_stencil) are accumulated.  cvcb_counters reads the totals and
+ * the number of kernels this context has launched (a graph launch counts
+ * its kernel nodes). */
+int cvcb_profile(cvcb_lattice *lat, int enable);
+int cvcb_counters(cvcb_lattice *lat, long long *kernel_launches, long long *stencil_launches_timed,
+                  double *stencil_ms, double *stencil_bytes);
 
 /* ---------------------------------------------------------------------
  * Contractions
