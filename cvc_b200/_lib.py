@@ -76,6 +76,7 @@ SIGNATURES = {
     "cvcb_mul_one_pm_imu_inv": (_I, [_P, _P, _D, _I]),
     "cvcb_spinor_scalar_product_co": (_I, [_P, _P, _P, _P, _I]),
     "cvcb_spinor_scalar_product_re": (_I, [_P, _P, _P, _P, _I]),
+    "cvcb_spinor_scalar_product_co_noalloc": (_I, [_I, _P, _P, _P, _I, _P]),
     "cvcb_invert_Qtm": (_I, [_P, _P, _P, _D, _I, _P]),
     "cvcb_invert_Qtm_her": (_I, [_P, _P, _P, _D, _I, _P]),
     "cvcb_solver_defaults": (None, [ctypes.POINTER(SolverParams)]),

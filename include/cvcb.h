@@ -149,6 +149,22 @@ int cvcb_mul_one_pm_imu_inv(cvcb_lattice *lat, double *phi, double sign, int V);
  * double *xi, double *phi, int V) (invert_Qtm.h:10). */
 int cvcb_spinor_scalar_product_co(cvcb_lattice *lat, double *w, const double *xi,
                                   const double *phi, int V);
+/* The same complex scalar product for callers that cannot allocate device
+ * memory (their device memory belongs to a pool of their own, or a
+ * cudaMalloc would synchronise a device they keep busy): no context is
+ * needed and nothing is allocated.  No counterpart in the reference.
+ * xi, phi (24*V doubles each) and w (2 doubles) are device memory of
+ * `device`; stream is a cudaStream_t (NULL: the legacy default stream).
+ * Stream-ordered: returns after enqueueing; w is ready when the stream
+ * reaches the call.  Scratch is one fixed device array per GPU (about
+ * 256 KB, held until the process exits), so V is limited to 5,592,405
+ * sites; larger V returns CVCB_ERR_ARG.  All calls on a device share that
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on a device looks up the array's address; make it
+ * before any stream capture on that device. */
+int cvcb_spinor_scalar_product_co_noalloc(int device, double *w, const double *xi,
+                                          const double *phi, int V, void *stream);
+
 /* r = Re sum_x xi(x)^dagger phi(x).  Replaces void
  * spinor_scalar_product_re(double *r, double *xi, double *phi, int V)
  * (invert_Qtm.h:9). */
