@@ -11,8 +11,9 @@
 //   FP16 spinor : uint4   s[3][stride] (8 halves each) + float norm[stride]
 //   FP64 links  : double2 U[4][9][V], boundary phase already multiplied in
 //                 (the reference multiplies it per use, Q_phi.c:66).
-//   FP32 links  : float4  U[4][3][V], rows 0 and 1 of the raw SU(3) link;
-//                 row 2 is rebuilt and the phase applied in registers.
+//   FP32 links  : float4  U[4][3][V], rows 0 and 1 of the phased link
+//                 e^{i theta} U; row 2 = e^{3 i theta} conj(row0 x row1) is
+//                 rebuilt in registers.
 //   FP16 links  : uint2   U[4][3][V], same 12 reals in half precision.
 #pragma once
 
@@ -61,6 +62,33 @@ const char *last_error();
     if (r_ < 0) return r_;         \
   } while (0)
 
+// ---- division by an invariant integer --------------------------------------
+// q = n / d as (umulhi(n, m) + n) >> s with s = ceil(log2 d) and
+// m = floor(2^32 (2^s - d) / d) + 1 (Granlund and Montgomery, "Division by
+// invariant integers using multiplication", PLDI 1994); exact for
+// 0 <= n < 2^31, which covers every site index here.
+struct FastDiv {
+  unsigned d, m, s;
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+  FastDiv f;
+  f.d = d;
+  f.s = 0;
+  while ((1u << f.s) < d) ++f.s;
+  f.m = (unsigned)((((unsigned long long)1 << 32) * (((unsigned long long)1 << f.s) - d)) / d + 1);
+  return f;
+}
+
+__host__ __device__ inline unsigned fdiv(unsigned n, const FastDiv &f) {
+#ifdef __CUDA_ARCH__
+  const unsigned t = __umulhi(n, f.m);
+#else
+  const unsigned t = (unsigned)(((unsigned long long)n * f.m) >> 32);
+#endif
+  return (t + n) >> f.s;
+}
+
 // ---- geometry passed to kernels by value ----------------------------------
 struct Geom {
   int T, LX, LY, LZ;
@@ -68,6 +96,7 @@ struct Geom {
   int s1;  // LZ             : lex step of +y
   int s2;  // LY*LZ          : lex step of +x
   int s3;  // LX*LY*LZ       : lex step of +t
+  FastDiv dLX, dLY, dLZ;
 };
 
 // Lexicographic coordinates of the even/odd site (p, i).
@@ -77,15 +106,16 @@ struct SiteCoord {
 
 __host__ __device__ inline SiteCoord site_coord(const Geom &g, int p, int i) {
   SiteCoord c;
-  const int m = 2 * i;
-  const int z0 = m % g.LZ;
-  int r = m / g.LZ;
-  c.y = r % g.LY;
-  r /= g.LY;
-  c.x = r % g.LX;
-  c.t = r / g.LX;
+  const unsigned m = 2u * (unsigned)i;
+  const unsigned r0 = fdiv(m, g.dLZ);
+  const int z0 = (int)(m - r0 * (unsigned)g.LZ);
+  const unsigned r1 = fdiv(r0, g.dLY);
+  c.y = (int)(r0 - r1 * (unsigned)g.LY);
+  const unsigned r2 = fdiv(r1, g.dLX);
+  c.x = (int)(r1 - r2 * (unsigned)g.LX);
+  c.t = (int)r2;
   c.z = z0 + ((p + c.t + c.x + c.y) & 1);
-  c.lex = m - z0 + c.z;
+  c.lex = (int)m - z0 + c.z;
   return c;
 }
 

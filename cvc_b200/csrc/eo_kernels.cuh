@@ -107,9 +107,10 @@ struct F16Acc {
 };
 
 // ---- link accessors ---------------------------------------------------------
-// kPhased: the stored link already carries the boundary phase.  Otherwise the
-// raw SU(3) link is rebuilt from two rows and the phase is applied to the
-// product U h (forward) or U^+ h (backward, conjugate phase).
+// Every accessor returns the phased link W = e^{i theta_mu} U.  The 12-real
+// forms store rows 0, 1 of W; since W is SU(3) times a phase, row 2 is
+// e^{3 i theta_mu} conj(W_0 x W_1) (ph holds e^{3 i theta_mu}; the product is
+// skipped in directions without a phase).
 struct L64 {
   using R = double;
   static constexpr bool kPhased = true;
@@ -136,9 +137,16 @@ struct L32f {  // 18 reals, single, phased
   }
 };
 
-struct L32c {  // 12 reals, single, raw SU(3)
+__device__ __forceinline__ void apply_row2_phase(Link<float> &L, float2 ph) {
+  if (ph.x != 1.f || ph.y != 0.f) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) L.m[2][j] = cmul(L.m[2][j], cx(ph.x, ph.y));
+  }
+}
+
+struct L32c {  // 12 reals, single, phased rows 0 and 1
   using R = float;
-  static constexpr bool kPhased = false;
+  static constexpr bool kPhased = true;
   const float4 *U;
   size_t V;
   float2 ph[4];
@@ -151,13 +159,14 @@ struct L32c {  // 12 reals, single, raw SU(3)
       L.m[(2 * q + 1) / 3][(2 * q + 1) % 3] = cx(v.z, v.w);
     }
     reconstruct_row2(L);
+    apply_row2_phase(L, ph[mu]);
     return L;
   }
 };
 
-struct L16c {  // 12 reals, half, raw SU(3)
+struct L16c {  // 12 reals, half, phased rows 0 and 1
   using R = float;
-  static constexpr bool kPhased = false;
+  static constexpr bool kPhased = true;
   const uint2 *U;
   size_t V;
   float2 ph[4];
@@ -172,6 +181,7 @@ struct L16c {  // 12 reals, half, raw SU(3)
       L.m[(2 * q + 1) / 3][(2 * q + 1) % 3] = cx(b.x, b.y);
     }
     reconstruct_row2(L);
+    apply_row2_phase(L, ph[mu]);
     return L;
   }
 };

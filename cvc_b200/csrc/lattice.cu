@@ -128,16 +128,18 @@ __global__ void k_gauge_forms(const double2 *__restrict__ raw, Geom g, double4 p
     double2 u[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) u[k] = raw[((size_t)lex * 4 + mu) * 9 + k];
+    double2 w[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
       // (re*pr - im*pi, re*pi + im*pr): the rounding of _cm_eq_cm_ti_co
-      const double2 v = cmul(u[k], ph[mu]);
-      U64[((size_t)mu * 9 + k) * g.V + eo] = v;
-      U32f[((size_t)mu * 9 + k) * g.V + eo] = make_float2((float)v.x, (float)v.y);
+      w[k] = cmul(u[k], ph[mu]);
+      U64[((size_t)mu * 9 + k) * g.V + eo] = w[k];
+      U32f[((size_t)mu * 9 + k) * g.V + eo] = make_float2((float)w[k].x, (float)w[k].y);
     }
+    // 12-real forms: rows 0 and 1 of the phased link
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      const double2 a = u[2 * q], b = u[2 * q + 1];
+      const double2 a = w[2 * q], b = w[2 * q + 1];
       U32c[((size_t)mu * 3 + q) * g.V + eo] =
           make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
       __half2 h0 = __floats2half2_rn((float)a.x, (float)a.y);
@@ -246,6 +248,9 @@ int cvcb_lattice_create(cvcb_lattice **out, int T, int LX, int LY, int LZ, int d
   L->g.s1 = LZ;
   L->g.s2 = LY * LZ;
   L->g.s3 = LX * LY * LZ;
+  L->g.dLX = make_fastdiv(LX);
+  L->g.dLY = make_fastdiv(LY);
+  L->g.dLZ = make_fastdiv(LZ);
   boundary_phases(T, LX, LY, LZ, L->bc, L->phase);
   cudaError_t e = cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&L->partials, kMaxRedBlocks * 4 * sizeof(double));

@@ -236,6 +236,21 @@ struct EpiRR {
   }
 };
 
+// sloppy <- FP64 (rhs with skip[r] == 0)
+template <class SF>
+__global__ void k_to_sloppy(SF dst, F64Acc src, const int *skip, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (s >= nsites || r >= nrhs || (skip && skip[r])) return;
+  dst.store(r, s, convert<typename SF::R>(src.load(r, s)));
+}
+
+template <class SF>
+struct RedNormS {
+  SF v;
+  __device__ double operator()(int r, int s) const { return norm2(v.load(r, s)); }
+};
+
 // copy r_s into p (restart of the direction)
 template <class SF>
 __global__ void k_copy(SF dst, SF src, const int *skip, int nsites, int nrhs) {
@@ -317,7 +332,7 @@ struct Batch {
   Geom g;
   LaunchShape shape;
   // FP64 fields: full lattice, stride V, rhs stride 12V
-  double2 *b64, *x64, *t64, *y64, *bh64, *rn64;
+  double2 *b64, *x64, *t64, *y64, *bh64;
   // sloppy fields: half lattice, compact
   SF p, Ap, rs, te, yo, te2;
   XF xs;
@@ -428,17 +443,18 @@ struct Batch {
     return hop<F64Acc, L64, false, false, true>(f64(out, 1), f64(t64, 0), f64(in, 1), links64, 1,
                                                 skip, 1, 0, ka(), m, 0.5);
   }
-  // FP64: out_o = M(mu)^+ in_o = g5 M(-mu) g5 in_o
-  int schur64_dag(double2 *out, double2 *in, const int *skip) {
-    double ia, ib;
-    ainv(-mu, ia, ib);
-    CVCB_TRY((hop<F64Acc, L64, true, false, false>(f64(t64, 0), f64(in, 1), f64(in, 1), links64, 0,
-                                                   skip, ia, ib, 0, 0, -0.5)));
-    return hop<F64Acc, L64, false, true, true>(f64(out, 1), f64(t64, 0), f64(in, 1), links64, 1,
-                                               skip, 1, 0, ka(), -mu, 0.5);
+  // sloppy: out_o = M(mu)^+ in_o = g5 M(-mu) g5 in_o (te2 as intermediate)
+  int dag_sloppy(SF out, SF in, const int *skip) {
+    double ja, jb;
+    ainv(-mu, ja, jb);
+    CVCB_TRY((hop<SF, LF, true, false, false>(te2, in, in, links, 0, skip, ja, jb, 0, 0, -0.5)));
+    return hop<SF, LF, false, true, true>(out, te2, in, links, 1, skip, 1, 0, ka(), -mu, 0.5);
   }
 
-  // r_hat = b_hat - M x64; rhat2 = |r_hat|^2; r_N = M^+ r_hat; r_s = r_N; rr = |r_N|^2
+  // Reliable update (rhs with ru_skip[r] == 0): x64 += x_s; r_hat = b_hat - M x64
+  // and |r_hat|^2 in FP64 with the exact operator (the convergence criterion);
+  // then the sloppy recursion restarts from r_s = M^+ r_hat, which only feeds
+  // the sloppy iterations and is therefore formed in sloppy precision.
   int reliable_update(bool absorb) {
     dim3 eg((g.Vh + 127) / 128, n);
     if (absorb) {
@@ -450,9 +466,10 @@ struct Batch {
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedRhat{f64(bh64, 1), f64(y64, 1)},
                                                     EpiStore{S.rhat2}, g.Vh, br, ru_skip);
     CVCB_LAUNCHED(L);
-    CVCB_TRY(schur64_dag(rn64, y64, ru_skip));
-    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedToSloppy<SF>{f64(rn64, 1), rs}, EpiRR{S},
-                                                    g.Vh, br, ru_skip);
+    k_to_sloppy<<<eg, 128, 0, L->stream>>>(yo, f64(y64, 1), ru_skip, g.Vh, n);
+    CVCB_LAUNCHED(L);
+    CVCB_TRY(dag_sloppy(rs, yo, ru_skip));
+    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedNormS<SF>{rs}, EpiRR{S}, g.Vh, br, ru_skip);
     CVCB_LAUNCHED(L);
     return CVCB_OK;
   }
@@ -491,10 +508,17 @@ L64 make_links<L64>(cvcb_lattice *L) {
   for (int m = 0; m < 4; ++m) l.ph[m] = make_double2(L->phase[2 * m], L->phase[2 * m + 1]);
   return l;
 }
+// e^{3 i theta_mu}: row 2 of a phased SU(3) link W = e^{i theta} U is
+// e^{3 i theta} conj(W_0 x W_1)
+static float2 phase_cubed(const cvcb_lattice *L, int m) {
+  const double c = L->phase[2 * m], d = L->phase[2 * m + 1];
+  const double c2 = c * c - d * d, d2 = 2 * c * d;
+  return make_float2((float)(c2 * c - d2 * d), (float)(c2 * d + d2 * c));
+}
 template <>
 L32c make_links<L32c>(cvcb_lattice *L) {
   L32c l{L->U32c, (size_t)L->g.V, {}};
-  for (int m = 0; m < 4; ++m) l.ph[m] = make_float2((float)L->phase[2 * m], (float)L->phase[2 * m + 1]);
+  for (int m = 0; m < 4; ++m) l.ph[m] = phase_cubed(L, m);
   return l;
 }
 template <>
@@ -506,7 +530,7 @@ L32f make_links<L32f>(cvcb_lattice *L) {
 template <>
 L16c make_links<L16c>(cvcb_lattice *L) {
   L16c l{L->U16c, (size_t)L->g.V, {}};
-  for (int m = 0; m < 4; ++m) l.ph[m] = make_float2((float)L->phase[2 * m], (float)L->phase[2 * m + 1]);
+  for (int m = 0; m < 4; ++m) l.ph[m] = phase_cubed(L, m);
   return l;
 }
 
@@ -533,7 +557,7 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   const size_t nrm = sizeof(float) * (size_t)g.Vh * n;
   const size_t scal = (6 * sizeof(double) + 2 * sizeof(int)) * kMaxBatch + 64;
   const size_t part = sizeof(double) * kMaxRedBlocks * kMaxBatch + sizeof(unsigned) * kMaxBatch;
-  const size_t total = 6 * f64 + 6 * (sl + nrm) + (xsl + nrm) + scal + part + 4096;
+  const size_t total = 5 * f64 + 6 * (sl + nrm) + (xsl + nrm) + scal + part + 4096;
   void *mem;
   CVCB_TRY(ensure_buffer(L, SLOT_MIX0, total, &mem));
   char *p = static_cast<char *>(mem);
@@ -547,7 +571,6 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   B.t64 = (double2 *)take(f64);
   B.y64 = (double2 *)take(f64);
   B.bh64 = (double2 *)take(f64);
-  B.rn64 = (double2 *)take(f64);
   SF *sl_fields[6] = {&B.p, &B.Ap, &B.rs, &B.te, &B.yo, &B.te2};
   for (SF *f : sl_fields) {
     void *b = take(sl);
