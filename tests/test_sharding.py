@@ -1,0 +1,85 @@
+"""The multi-rank path on CPU: two gloo ranks shard source positions and
+gather Pi_mu_nu; the result must equal the single-process run bit for bit.
+The per-source computation here is the oracle's contraction on a small
+lattice (the CUDA library is not needed to test the host orchestration)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+from golden import inputs
+
+DIMS, V = (4, 2, 2, 2), 32
+SOURCES = [0, 3, 5, 17, 30]
+
+
+def pi_for_source(src):
+    import oracle_bind as ob
+    o = ob.Oracle(*DIMS, 0.15, 0.03)
+    o.set_gauge(inputs.gauge(9, V))
+    fields = [inputs.field(1000 * (src + 1) + i, 24 * V) for i in range(120)]
+    conn, _ = o.cvc_contract(fields, src)
+    return conn
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank_main(rank, world, port, q):
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, here)
+    sys.path.insert(0, os.path.dirname(here))
+    import torch.distributed as dist
+    from cvc_b200 import sharding
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        res = sharding.run_sharded(SOURCES, pi_for_source)
+        mine = sharding.my_items(range(len(SOURCES)), world, rank)
+        local = [torch.from_numpy(pi_for_source(SOURCES[i])) for i in mine]
+        stacked = sharding.gather_tensors(local, len(SOURCES))
+        tmax = sharding.max_over_ranks(1.0 + rank)
+        q.put((rank, {k: v for k, v in res.items()}, stacked.numpy(), tmax, mine))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_partition_covers_each_item_once():
+    from cvc_b200 import sharding
+    for world in (1, 2, 3, 8):
+        seen = []
+        for r in range(world):
+            seen += sharding.my_items(range(13), world, r)
+        assert sorted(seen) == list(range(13))
+
+
+def test_two_gloo_ranks_match_single_process(oracle_mod):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=240) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    serial = {s: pi_for_source(s) for s in SOURCES}
+    for rank, res, stacked, tmax, mine in out:
+        assert tmax == 2.0
+        assert set(res) == set(SOURCES)
+        for s in SOURCES:
+            assert np.array_equal(res[s], serial[s])
+        for i, s in enumerate(SOURCES):
+            assert np.array_equal(stacked[i], serial[s])
+    assert sorted(out[0][4] + out[1][4]) == list(range(len(SOURCES)))
