@@ -89,6 +89,9 @@ SIGNATURES = {
     "cvcb_cvc_ward": (_I, [_P, _P, _P]),
     "cvcb_p2gg_seq_source": (_I, [_P, _P, _P, _I, _P, _I, _I]),
     "cvcb_plaquette": (_I, [_P, _P, _P]),
+    "cvcb_pi_forward": (_I, [_P, _I, ctypes.POINTER(SolverParams), _D, _P, _P]),
+    "cvcb_pi_tangent": (_I, [_P, _I, _P]),
+    "cvcb_pi_backward": (_I, [_P, _P, _P, _P, _P]),
 }
 
 _lib = None

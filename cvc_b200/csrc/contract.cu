@@ -20,18 +20,12 @@
 #include <vector>
 
 #include "cvcb_internal.h"
+#include "contract_plan.h"
 #include "reduce.cuh"
 #include "spinor_ops.cuh"
 
 namespace cvcb {
 
-struct ZTerm {
-  int src;       // column of the dn block (0..59 within fields[60..119])
-  double2 coef;  // conj(k us)
-};
-struct ZPlan {
-  ZTerm t[24][6];  // 24 columns (2 parts x 12), 6 terms each
-};
 
 // Z columns of one nu: thread per site, reads 12 or 24 dn columns, writes 24.
 __global__ void __launch_bounds__(128) k_cvc_z(double2 *__restrict__ Z,
@@ -250,6 +244,90 @@ struct LinkSumF {
   }
 };
 
+// Coefficient plans of the Z columns for the four nu (see the file comment),
+// and the phased source links Usource[nu] (cvc_exact2_xspace.c:293-304).
+int make_zplans(cvcb_lattice *L, int src, ZPlan plans[4], double Us[4][18], ZMeta *meta) {
+  // the reference's gamma bookkeeping (cvc_exact2_xspace.c:336-383)
+  int perm[16][24], sign[16][24];
+  gamma_tables(perm, sign);
+  int gperm[5][4], isimag[4];
+  double gsign[5][4];
+  for (int ir = 0; ir < 4; ++ir) {
+    gperm[4][ir] = perm[5][6 * ir] / 6;
+    gsign[4][ir] = sign[5][6 * ir];
+  }
+  for (int nu = 0; nu < 4; ++nu) {
+    for (int ir = 0; ir < 4; ++ir) {
+      gperm[nu][ir] = perm[6 + nu][6 * ir] / 6;
+      gsign[nu][ir] = sign[6 + nu][6 * ir];
+    }
+    isimag[nu] = perm[6 + nu][0] % 2;
+  }
+  // phased source links Usource[nu] (:293-304)
+  const double *G = L->gauge_host.data();
+  for (int nu = 0; nu < 4; ++nu)
+    for (int k = 0; k < 9; ++k) {
+      const double re = G[18 * (4 * (size_t)src + nu) + 2 * k],
+                   im = G[18 * (4 * (size_t)src + nu) + 2 * k + 1];
+      const double pr = L->phase[2 * nu], pi = L->phase[2 * nu + 1];
+      Us[nu][2 * k] = re * pr - im * pi;
+      Us[nu][2 * k + 1] = re * pi + im * pr;
+    }
+
+  for (int nu = 0; nu < 4; ++nu) {
+    ZPlan &plan = plans[nu];
+    for (int part = 0; part < 2; ++part)
+      for (int ir = 0; ir < 4; ++ir)
+        for (int ia = 0; ia < 3; ++ia) {
+          const int col = part * 12 + 3 * ir + ia;
+          int q = 0;
+          for (int gg = 0; gg < 2; ++gg) {
+            const int gi = gg == 0 ? nu : 4;
+            // k: +-1 or +-i
+            double kr, ki;
+            if (gg == 0) {
+              kr = isimag[nu] ? 0.0 : gsign[nu][ir];
+              ki = isimag[nu] ? -gsign[nu][ir] : 0.0;
+            } else {
+              kr = part == 0 ? -gsign[4][ir] : gsign[4][ir];
+              ki = 0.0;
+            }
+            for (int ib = 0; ib < 3; ++ib) {
+              double ur, ui;  // us
+              if (part == 0) {
+                ur = Us[nu][2 * (3 * ia + ib)];
+                ui = Us[nu][2 * (3 * ia + ib) + 1];
+              } else {
+                ur = Us[nu][2 * (3 * ib + ia)];
+                ui = -Us[nu][2 * (3 * ib + ia) + 1];
+              }
+              const double cr = kr * ur - ki * ui, ci = kr * ui + ki * ur;
+              const int d = 3 * gperm[gi][ir] + ib;
+              // chi: part 0 -> dn shifted by nu (block nu), part 1 -> dn unshifted (block 4)
+              plan.t[col][q].src = (part == 0 ? nu * 12 : 48) + d;
+              plan.t[col][q].coef = make_double2(cr, -ci);
+              if (meta) {
+                ZMeta &m = meta[(nu * 24 + col) * 6 + q];
+                m.k = make_double2(kr, ki);
+                m.ia = ia;
+                m.ib = ib;
+                m.part = part;
+              }
+              ++q;
+            }
+          }
+        }
+  }
+  return CVCB_OK;
+}
+
+// Z columns of one nu into Z (24 fields), from the 60 dn fields at dn.
+int launch_cvc_z(cvcb_lattice *L, double2 *Z, const double2 *dn, const ZPlan &plan) {
+  k_cvc_z<<<(L->g.V + 127) / 128, 128, 0, L->stream>>>(Z, dn, plan, L->g.V);
+  CVCB_LAUNCHED(L);
+  return CVCB_OK;
+}
+
 static int need_gauge(cvcb_lattice *L) {
   if (!L->have_gauge) {
     set_error("no gauge field uploaded");
@@ -285,71 +363,14 @@ int cvc_contract(cvcb_lattice *L, const double *const *fields, int src, double *
   double2 *P = static_cast<double2 *>(props);
   for (int f = 0; f < 120; ++f) CVCB_TRY(spinor_in(L, P + f * fs, fields[f], g.V));
 
-  // reference's gamma bookkeeping (cvc_exact2_xspace.c:336-383)
+  ZPlan plans[4];
+  double Us[4][18];
   int perm[16][24], sign[16][24];
   gamma_tables(perm, sign);
-  int gperm[5][4], isimag[4];
-  double gsign[5][4];
-  for (int ir = 0; ir < 4; ++ir) {
-    gperm[4][ir] = perm[5][6 * ir] / 6;
-    gsign[4][ir] = sign[5][6 * ir];
-  }
-  for (int nu = 0; nu < 4; ++nu) {
-    for (int ir = 0; ir < 4; ++ir) {
-      gperm[nu][ir] = perm[6 + nu][6 * ir] / 6;
-      gsign[nu][ir] = sign[6 + nu][6 * ir];
-    }
-    isimag[nu] = perm[6 + nu][0] % 2;
-  }
-  // phased source links Usource[nu] (:293-304)
-  double Us[4][18];
-  const double *G = L->gauge_host.data();
-  for (int nu = 0; nu < 4; ++nu)
-    for (int k = 0; k < 9; ++k) {
-      const double re = G[18 * (4 * (size_t)src + nu) + 2 * k],
-                   im = G[18 * (4 * (size_t)src + nu) + 2 * k + 1];
-      const double pr = L->phase[2 * nu], pi = L->phase[2 * nu + 1];
-      Us[nu][2 * k] = re * pr - im * pi;
-      Us[nu][2 * k + 1] = re * pi + im * pr;
-    }
-
+  make_zplans(L, src, plans, Us, nullptr);
   const int blocks = (g.V + 127) / 128;
   for (int nu = 0; nu < 4; ++nu) {
-    ZPlan plan;
-    for (int part = 0; part < 2; ++part)
-      for (int ir = 0; ir < 4; ++ir)
-        for (int ia = 0; ia < 3; ++ia) {
-          const int col = part * 12 + 3 * ir + ia;
-          int q = 0;
-          for (int gg = 0; gg < 2; ++gg) {
-            const int gi = gg == 0 ? nu : 4;
-            // k: +-1 or +-i
-            double kr, ki;
-            if (gg == 0) {
-              kr = isimag[nu] ? 0.0 : gsign[nu][ir];
-              ki = isimag[nu] ? -gsign[nu][ir] : 0.0;
-            } else {
-              kr = part == 0 ? -gsign[4][ir] : gsign[4][ir];
-              ki = 0.0;
-            }
-            for (int ib = 0; ib < 3; ++ib) {
-              double ur, ui;  // us
-              if (part == 0) {
-                ur = Us[nu][2 * (3 * ia + ib)];
-                ui = Us[nu][2 * (3 * ia + ib) + 1];
-              } else {
-                ur = Us[nu][2 * (3 * ib + ia)];
-                ui = -Us[nu][2 * (3 * ib + ia) + 1];
-              }
-              const double cr = kr * ur - ki * ui, ci = kr * ui + ki * ur;
-              const int d = 3 * gperm[gi][ir] + ib;
-              // chi: part 0 -> dn shifted by nu (block nu), part 1 -> dn unshifted (block 4)
-              plan.t[col][q].src = (part == 0 ? nu * 12 : 48) + d;
-              plan.t[col][q].coef = make_double2(cr, -ci);
-              ++q;
-            }
-          }
-        }
+    const ZPlan &plan = plans[nu];
     k_cvc_z<<<blocks, 128, 0, L->stream>>>(static_cast<double2 *>(zb), P + 60 * fs, plan, g.V);
     CVCB_LAUNCHED(L);
     k_cvc_pi<<<blocks, 128, 0, L->stream>>>(static_cast<double *>(cb), P + 48 * fs,

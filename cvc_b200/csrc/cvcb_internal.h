@@ -261,6 +261,12 @@ int p2gg_seq_source(cvcb_lattice *L, double *source, const double *prop, int t, 
                     int gamma_id, int pos);
 int plaquette(cvcb_lattice *L, double *plaq, double *linksum);
 
+// adjoint.cu
+int pi_forward(cvcb_lattice *L, int src, const cvcb_solver_params *P, double keep_bytes,
+               double *conn, double *contact);
+int pi_tangent(cvcb_lattice *L, int param, double *dconn);
+int pi_backward(cvcb_lattice *L, const double *wts, double *dLdU, double *dLdmu, double *dLdkappa);
+
 // solver_mixed.cu
 int time_stencil(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int reps, double *ms);
 int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int nrhs,

@@ -224,6 +224,37 @@ class Lattice:
             self._h, ptr(source), ptr(prop), int(timeslice), ptr(mom), int(gamma_id),
             int(propagator_position)))
 
+    # -- derivatives of Pi (no counterpart in the reference) -------------
+    def pi_forward(self, source_site, params=None, keep_bytes=float("inf"), conn=None):
+        """Solve the 120 columns of source point y and contract: (conn, contact)."""
+        if params is None:
+            params = solver_defaults()
+        if conn is None:
+            conn = np.zeros(32 * self.VOLUME)
+        contact = np.zeros(8)
+        kb = 1e300 if keep_bytes == float("inf") else float(keep_bytes)
+        _check("pi_forward", self._lib.cvcb_pi_forward(self._h, int(source_site),
+                                                        ctypes.byref(params), kb, ptr(conn),
+                                                        ptr(contact)))
+        return conn, contact
+
+    def pi_tangent(self, parameter):
+        """dPi/dmu (parameter 'mu') or dPi/dkappa ('kappa') at the last forward state."""
+        code = {"mu": 0, "kappa": 1}[parameter]
+        d = np.zeros(32 * self.VOLUME)
+        _check("pi_tangent", self._lib.cvcb_pi_tangent(self._h, code, ptr(d)))
+        return d
+
+    def pi_backward(self, weights, want_gauge=True):
+        """For L = Re sum conj(w) Pi: (dL/dmu, dL/dkappa, dL/dU or None)."""
+        w = np.ascontiguousarray(weights, np.float64)
+        dmu = np.zeros(1)
+        dka = np.zeros(1)
+        gu = np.zeros(72 * self.VOLUME) if want_gauge else None
+        _check("pi_backward", self._lib.cvcb_pi_backward(self._h, ptr(w), ptr(gu), ptr(dmu),
+                                                          ptr(dka)))
+        return float(dmu[0]), float(dka[0]), gu
+
     def plaquette(self):
         pl = np.zeros(1)
         ls = np.zeros(2)

@@ -285,6 +285,34 @@ int cvcb_cvc_ward(cvcb_lattice *lat, const double *conn, double *wi);
 int cvcb_p2gg_seq_source(cvcb_lattice *lat, double *source, const double *prop, int timeslice,
                          const int momentum[3], int gamma_id, int propagator_position);
 
+/* ---------------------------------------------------------------------
+ * Derivatives of Pi_mu_nu.  No counterpart in the reference.
+ * ------------------------------------------------------------------- */
+
+/* Forward pass: solves the 120 propagator columns of source point y
+ * (up = Q(mu)^-1, dn = Q(-mu)^-1, point sources at y + mu-hat for mu =
+ * 0..3 and at y, column order as cvcb_cvc_contract expects) with the
+ * batched solver under `params`, and returns Pi_mu_nu (and the contact
+ * term, may be NULL).  The columns are kept on the GPU for the calls below
+ * when they need at most keep_bytes of device memory (120 * 192 * V bytes);
+ * otherwise they are recomputed when needed. */
+int cvcb_pi_forward(cvcb_lattice *lat, int source_site, const cvcb_solver_params *params,
+                    double keep_bytes, double *conn, double *contact);
+
+/* Tangent: dPi_mu_nu / d parameter for parameter 0 = mu (the bare twisted
+ * mass g_mu) or 1 = kappa, at the state of the last forward pass (one extra
+ * solve per column).  dconn: 32*V doubles, the layout of conn. */
+int cvcb_pi_tangent(cvcb_lattice *lat, int parameter, double *dconn);
+
+/* Backward (adjoint) pass for L = Re sum_{x,mu,nu} conj(w_munu(x))
+ * Pi_munu(x), weights in the layout of conn (32*V doubles).  Returns
+ * dL/dmu, dL/dkappa and, if dL_dU is not NULL, the gradient with respect to
+ * the raw gauge links (72*V doubles, CVC gauge layout): for every link entry
+ * U_ab the pair (dL/dRe U_ab, dL/dIm U_ab).  One adjoint solve per column
+ * (Q(mu)^-dagger = g5 Q(-mu)^-1 g5). */
+int cvcb_pi_backward(cvcb_lattice *lat, const double *weights, double *dL_dU, double *dL_dmu,
+                     double *dL_dkappa);
+
 /* Plaquette <Re tr U_munu>/(18 V) and link sum (cvc_utils.c:384-436). */
 int cvcb_plaquette(cvcb_lattice *lat, double *plaq, double *linksum);
 
