@@ -89,6 +89,9 @@ struct F16Acc {
 #pragma unroll
     for (int c = 0; c < 12; ++c)
       mx = fmaxf(mx, fmaxf(fabsf(s.c[c / 3][c % 3].re), fabsf(s.c[c / 3][c % 3].im)));
+    // A site whose largest component is below the smallest normal float
+    // (far from a point source) is stored as zero: 1/mx would overflow.
+    if (!(mx >= 1.17549435e-38f)) mx = 0.f;
     const float inv = mx > 0.f ? 1.f / mx : 0.f;
     uint4 *q = p + r * rstride + j;
 #pragma unroll

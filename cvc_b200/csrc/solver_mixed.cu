@@ -102,8 +102,13 @@ __device__ __forceinline__ Spinor<R> convert(const Spinor<S> &a) {
   return o;
 }
 
+// The sloppy recursion works in units of the last true residual: sloppy
+// fields = scale * (true fields), scale = 1 / |r_hat| from the latest
+// reliable update, so its magnitudes stay O(1) whatever the size of b
+// (a source of 1e-33 would otherwise reach FP32 denormals).
 struct Scal {  // per right-hand side, device arrays
   double *rr, *pAp, *alpha, *beta, *rhat2, *rn2;
+  double *scale, *scale_prev;
   int *done;
 };
 
@@ -176,13 +181,15 @@ __global__ void k_p_upd(SF p, SF rs, Scal S, int nsites, int nrhs) {
   p.store(r, s, pv);
 }
 
-// Reliable update, step 1: x64 += x_s; x_s = 0 (rhs with skip[r] == 0)
+// Reliable update, step 1: x64 += x_s / scale; x_s = 0 (rhs with skip[r] == 0)
 template <class XF>
-__global__ void k_absorb(F64Acc x64, XF xs, const int *skip, int nsites, int nrhs) {
+__global__ void k_absorb(F64Acc x64, XF xs, const double *scale, const int *skip, int nsites,
+                         int nrhs) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int r = blockIdx.y;
   if (s >= nsites || r >= nrhs || skip[r]) return;
   using RX = typename XF::R;
+  const double w = 1.0 / scale[r];
   Spinor<double> xv = x64.load(r, s);
   const Spinor<RX> d = xs.load(r, s);
   Spinor<RX> z;
@@ -190,8 +197,8 @@ __global__ void k_absorb(F64Acc x64, XF xs, const int *skip, int nsites, int nrh
   for (int k = 0; k < 4; ++k)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      xv.c[k][c].re += (double)d.c[k][c].re;
-      xv.c[k][c].im += (double)d.c[k][c].im;
+      xv.c[k][c].re = fma(w, (double)d.c[k][c].re, xv.c[k][c].re);
+      xv.c[k][c].im = fma(w, (double)d.c[k][c].im, xv.c[k][c].im);
       z.c[k][c] = cx((RX)0, (RX)0);
     }
   x64.store(r, s, xv);
@@ -216,18 +223,16 @@ struct EpiStore {
   double *dst;
   __device__ void operator()(int r, double t) const { dst[r] = t; }
 };
-
-// r_s = sloppy(r_N); returns |r_N|^2 (FP64)
-template <class SF>
-struct RedToSloppy {
-  F64Acc rN;
-  SF rs;
-  __device__ double operator()(int r, int s) const {
-    const Spinor<double> v = rN.load(r, s);
-    rs.store(r, s, convert<typename SF::R>(v));
-    return norm2(v);
+// |r_hat|^2, and the new unit of the sloppy recursion
+struct EpiRhat {
+  Scal S;
+  __device__ void operator()(int r, double t) const {
+    S.rhat2[r] = t;
+    S.scale_prev[r] = S.scale[r];
+    S.scale[r] = (t > 0 && isfinite(t)) ? rsqrt(t) : 1.0;
   }
 };
+
 struct EpiRR {
   Scal S;
   __device__ void operator()(int r, double t) const {
@@ -238,11 +243,18 @@ struct EpiRR {
 
 // sloppy <- FP64 (rhs with skip[r] == 0)
 template <class SF>
-__global__ void k_to_sloppy(SF dst, F64Acc src, const int *skip, int nsites, int nrhs) {
+__global__ void k_to_sloppy(SF dst, F64Acc src, const double *scale, const int *skip, int nsites,
+                            int nrhs) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int r = blockIdx.y;
   if (s >= nsites || r >= nrhs || (skip && skip[r])) return;
-  dst.store(r, s, convert<typename SF::R>(src.load(r, s)));
+  Spinor<double> v = src.load(r, s);
+  const double w = scale[r];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v.c[k][c] = w * v.c[k][c];
+  dst.store(r, s, convert<typename SF::R>(v));
 }
 
 template <class SF>
@@ -250,6 +262,68 @@ struct RedNormS {
   SF v;
   __device__ double operator()(int r, int s) const { return norm2(v.load(r, s)); }
 };
+
+// Reliable update, direction kept: before r_s is replaced, q = p - r_s
+// (= beta p_prev of the last iteration) is kept in p ...
+template <class SF>
+__global__ void k_dir_strip(SF p, SF rs, const int *skip, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (s >= nsites || r >= nrhs || skip[r]) return;
+  using R = typename SF::R;
+  Spinor<R> pv = p.load(r, s);
+  const Spinor<R> rv = rs.load(r, s);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pv.c[k][c] = pv.c[k][c] - rv.c[k][c];
+  p.store(r, s, pv);
+}
+
+// ... and with the new residual r_s', p = r_s' + q - (<r_s', q> / |r_s'|^2) r_s':
+// q is made orthogonal to r_s' again, so that <r_s', p> = |r_s'|^2 as in
+// exact CG and the Krylov directions built so far are not thrown away.
+template <class SF>
+struct RedCdot {  // Re or Im of <a, b> = sum conj(a) b
+  SF a, b;
+  int imag;
+  __device__ double operator()(int r, int s) const {
+    const auto u = a.load(r, s), v = b.load(r, s);
+    double t = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        t += imag ? (double)u.c[k][c].re * v.c[k][c].im - (double)u.c[k][c].im * v.c[k][c].re
+                  : (double)u.c[k][c].re * v.c[k][c].re + (double)u.c[k][c].im * v.c[k][c].im;
+    return t;
+  }
+};
+template <class SF>
+__global__ void k_dir_restore(SF p, SF rs, Scal S, const int *skip, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (s >= nsites || r >= nrhs || skip[r]) return;
+  using R = typename SF::R;
+  // q was stored in the previous unit: q' = u q with u = scale / scale_prev,
+  // and <r_s', q'> = u <r_s', q> (the reductions ran on the unrescaled q)
+  const double u = S.scale[r] / S.scale_prev[r];
+  const double n2 = S.rr[r], cre = u * S.pAp[r], cim = u * S.alpha[r];
+  const bool ok = n2 > 0 && isfinite(n2) && isfinite(cre) && isfinite(cim) && isfinite(u);
+  const R a = (R)(ok ? 1.0 - cre / n2 : 1.0), b = (R)(ok ? cim / n2 : 0.0);
+  const R uq = (R)(ok ? u : 0.0);
+  Spinor<R> pv = p.load(r, s);
+  const Spinor<R> rv = rs.load(r, s);
+  // p = (a - i b) r_s' + u q
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const Cx<R> x = rv.c[k][c];
+      pv.c[k][c] = uq * pv.c[k][c] + cx(a * x.re + b * x.im, a * x.im - b * x.re);
+    }
+  p.store(r, s, pv);
+}
 
 // copy r_s into p (restart of the direction)
 template <class SF>
@@ -339,7 +413,8 @@ struct Batch {
   void *xs_mem;
   size_t xs_bytes;
   Scal S;
-  int *ru_skip;  // per rhs: 1 = skip in the reliable update
+  int *ru_skip;   // per rhs: 1 = skip in the reliable update
+  int *rst_skip;  // per rhs: 0 = restart the direction from the residual
   BatchRed br;
   LF links;
   L64 links64;
@@ -379,11 +454,15 @@ struct Batch {
       CVCB_CUDA(cudaEventCreate(&rec.b));
       CVCB_CUDA(cudaEventRecordWithFlags(rec.a, L->stream, capturing ? cudaEventRecordExternal : 0));
     }
-    switch (sh.nr) {
-      case 2: k_eo_hop<AF, LL, 2, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
-      case 3: k_eo_hop<AF, LL, 3, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
-      case 4: k_eo_hop<AF, LL, 4, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
-      default: k_eo_hop<AF, LL, 1, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
+    if constexpr (sizeof(typename AF::R) == 8) {
+      k_eo_hop<AF, LL, 1, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
+    } else {
+      switch (sh.nr) {
+        case 2: k_eo_hop<AF, LL, 2, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
+        case 3: k_eo_hop<AF, LL, 3, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
+        case 4: k_eo_hop<AF, LL, 4, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
+        default: k_eo_hop<AF, LL, 1, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
+      }
     }
     CVCB_LAUNCHED(L);
     if (rec_this) {
@@ -458,15 +537,15 @@ struct Batch {
   int reliable_update(bool absorb) {
     dim3 eg((g.Vh + 127) / 128, n);
     if (absorb) {
-      k_absorb<<<eg, 128, 0, L->stream>>>(f64(x64, 1), xs, ru_skip, g.Vh, n);
+      k_absorb<<<eg, 128, 0, L->stream>>>(f64(x64, 1), xs, S.scale, ru_skip, g.Vh, n);
       CVCB_LAUNCHED(L);
     }
     CVCB_TRY(schur64(y64, x64, mu, ru_skip));
     dim3 rg(red_blocks_sites(g.Vh), n);
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedRhat{f64(bh64, 1), f64(y64, 1)},
-                                                    EpiStore{S.rhat2}, g.Vh, br, ru_skip);
+                                                    EpiRhat{S}, g.Vh, br, ru_skip);
     CVCB_LAUNCHED(L);
-    k_to_sloppy<<<eg, 128, 0, L->stream>>>(yo, f64(y64, 1), ru_skip, g.Vh, n);
+    k_to_sloppy<<<eg, 128, 0, L->stream>>>(yo, f64(y64, 1), S.scale, ru_skip, g.Vh, n);
     CVCB_LAUNCHED(L);
     CVCB_TRY(dag_sloppy(rs, yo, ru_skip));
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedNormS<SF>{rs}, EpiRR{S}, g.Vh, br, ru_skip);
@@ -555,15 +634,17 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   const size_t sl = sloppy_site_bytes<SF>() * (size_t)g.Vh * n;
   const size_t xsl = sloppy_site_bytes<XF>() * (size_t)g.Vh * n;
   const size_t nrm = sizeof(float) * (size_t)g.Vh * n;
-  const size_t scal = (6 * sizeof(double) + 2 * sizeof(int)) * kMaxBatch + 64;
-  const size_t part = sizeof(double) * kMaxRedBlocks * kMaxBatch + sizeof(unsigned) * kMaxBatch;
-  const size_t total = 5 * f64 + 6 * (sl + nrm) + (xsl + nrm) + scal + part + 4096;
+  auto rnd = [](size_t b) { return (b + 255) & ~size_t(255); };  // every piece 256-aligned
+  const size_t scal = 8 * rnd(sizeof(double) * kMaxBatch) + 3 * rnd(sizeof(int) * kMaxBatch);
+  const size_t part = rnd(sizeof(double) * kMaxRedBlocks * kMaxBatch) +
+                      rnd(sizeof(unsigned) * kMaxBatch);
+  const size_t total = 5 * rnd(f64) + 6 * (rnd(sl) + rnd(nrm)) + rnd(xsl) + rnd(nrm) + scal + part;
   void *mem;
   CVCB_TRY(ensure_buffer(L, SLOT_MIX0, total, &mem));
   char *p = static_cast<char *>(mem);
   auto take = [&](size_t bytes) {
     char *q = p;
-    p += (bytes + 255) & ~size_t(255);
+    p += rnd(bytes);
     return q;
   };
   B.b64 = (double2 *)take(f64);
@@ -590,13 +671,17 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   B.S.beta = (double *)take(sizeof(double) * kMaxBatch);
   B.S.rhat2 = (double *)take(sizeof(double) * kMaxBatch);
   B.S.rn2 = (double *)take(sizeof(double) * kMaxBatch);
+  B.S.scale = (double *)take(sizeof(double) * kMaxBatch);
+  B.S.scale_prev = (double *)take(sizeof(double) * kMaxBatch);
   B.S.done = (int *)take(sizeof(int) * kMaxBatch);
   B.ru_skip = (int *)take(sizeof(int) * kMaxBatch);
+  B.rst_skip = (int *)take(sizeof(int) * kMaxBatch);
   B.br.partials = (double *)take(sizeof(double) * kMaxRedBlocks * kMaxBatch);
   B.br.counters = (unsigned *)take(sizeof(unsigned) * kMaxBatch);
   CVCB_CUDA(cudaMemsetAsync(B.br.counters, 0, sizeof(unsigned) * kMaxBatch, L->stream));
   CVCB_CUDA(cudaMemsetAsync(B.S.done, 0, sizeof(int) * kMaxBatch, L->stream));
   CVCB_CUDA(cudaMemsetAsync(B.ru_skip, 0, sizeof(int) * kMaxBatch, L->stream));
+  CVCB_CUDA(cudaMemsetAsync(B.S.scale, 0, 2 * rnd(sizeof(double) * kMaxBatch), L->stream));
   return CVCB_OK;
 }
 
@@ -715,7 +800,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, nullptr, g.Vh, n);
   CVCB_LAUNCHED(L);
   std::vector<double> rr(n), rr_max(n), rhat2(n), ratio2(n), target2(n);
-  std::vector<int> done(n, 0), iters(n, 0), since(n, 0), skip(n, 0);
+  std::vector<int> done(n, 0), iters(n, 0), since(n, 0), skip(n, 0), rst(n, 1);
   CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
   CVCB_CUDA(cudaMemcpyAsync(rhat2.data(), B.S.rhat2, n * sizeof(double), cudaMemcpyDeviceToHost,
                             L->stream));
@@ -775,7 +860,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   };
 
   const double delta2 = P->delta * P->delta;
-  int total_iter = 0, nru = 0;
+  int total_iter = 0, nru = 0, nrestart = 0;
   const double t0 = now_s();
   int rc = CVCB_OK;
   while (true) {
@@ -823,10 +908,32 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     if (!any) continue;
     CVCB_CUDA(cudaMemcpyAsync(B.ru_skip, skip.data(), n * sizeof(int), cudaMemcpyHostToDevice,
                               L->stream));
-    CVCB_TRY(B.reliable_update(true));
-    // restart the search direction of updated rhs from the true residual
-    k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.ru_skip, g.Vh, n);
+    // keep the search direction: q = p - r_s now, p = r_s' + q (q orthogonalised
+    // against r_s') after the update
+    k_dir_strip<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.ru_skip, g.Vh, n);
     CVCB_LAUNCHED(L);
+    CVCB_TRY(B.reliable_update(true));
+    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedCdot<SF>{B.rs, B.p, 0}, EpiStore{B.S.pAp},
+                                                    g.Vh, B.br, B.ru_skip);
+    CVCB_LAUNCHED(L);
+    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedCdot<SF>{B.rs, B.p, 1},
+                                                    EpiStore{B.S.alpha}, g.Vh, B.br, B.ru_skip);
+    CVCB_LAUNCHED(L);
+    k_dir_restore<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.S, B.ru_skip, g.Vh, n);
+    CVCB_LAUNCHED(L);
+    // a residual that stopped being finite restarts from the recomputed one
+    bool restart = false;
+    for (int i = 0; i < n; ++i) {
+      rst[i] = (skip[i] || std::isfinite(rr[i])) ? 1 : 0;
+      restart = restart || !rst[i];
+    }
+    if (restart) {
+      CVCB_CUDA(cudaMemcpyAsync(B.rst_skip, rst.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                                L->stream));
+      k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.rst_skip, g.Vh, n);
+      CVCB_LAUNCHED(L);
+      for (int i = 0; i < n; ++i) nrestart += !rst[i];
+    }
     ++nru;
     CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost,
                               L->stream));
@@ -876,6 +983,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   }
   st->iterations += std::accumulate(iters.begin(), iters.end(), 0);
   st->reliable_updates += nru;
+  st->restarts += nrestart;
   st->converged += nconv;
   st->max_true_res = std::max(st->max_true_res, worst);
   st->seconds += now_s() - t0;
@@ -883,7 +991,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
 }
 
 template <class SF, class XF, class LF>
-int time_stencil_t(cvcb_lattice *L, int prec, int recon, int nrhs, int reps, double *ms) {
+int time_stencil_t(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int reps, double *ms) {
   Batch<SF, XF, LF> B;
   CVCB_TRY(setup_batch(L, B, nrhs, /*with_fp64=*/false));
   // zero contents: timing of the stencil does not depend on the values
@@ -893,6 +1001,7 @@ int time_stencil_t(cvcb_lattice *L, int prec, int recon, int nrhs, int reps, dou
   double ia, ib;
   B.ainv(B.mu, ia, ib);
   auto one = [&] {
+    if (kind == 2) return B.normal_op_sloppy(B.Ap, B.p, nullptr);
     return B.template hop<SF, LF, false, false, false>(B.te, B.p, B.p, B.links, 0, nullptr, ia,
                                                        ib, 0, 0, -0.5);
   };
@@ -945,12 +1054,13 @@ int time_stencil(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int r
     *ms = t / reps;
     return CVCB_OK;
   }
-  if (prec == CVCB_PREC_DOUBLE) return time_stencil_t<F64Acc, F64Acc, L64>(L, prec, 18, nrhs, reps, ms);
+  if (prec == CVCB_PREC_DOUBLE)
+    return time_stencil_t<F64Acc, F64Acc, L64>(L, kind, prec, 18, nrhs, reps, ms);
   if (prec == CVCB_PREC_SINGLE)
-    return recon == 12 ? time_stencil_t<F32Acc, F32Acc, L32c>(L, prec, recon, nrhs, reps, ms)
-                       : time_stencil_t<F32Acc, F32Acc, L32f>(L, prec, recon, nrhs, reps, ms);
-  return recon == 12 ? time_stencil_t<F16Acc, F32Acc, L16c>(L, prec, recon, nrhs, reps, ms)
-                     : time_stencil_t<F16Acc, F32Acc, L32f>(L, prec, recon, nrhs, reps, ms);
+    return recon == 12 ? time_stencil_t<F32Acc, F32Acc, L32c>(L, kind, prec, recon, nrhs, reps, ms)
+                       : time_stencil_t<F32Acc, F32Acc, L32f>(L, kind, prec, recon, nrhs, reps, ms);
+  return recon == 12 ? time_stencil_t<F16Acc, F32Acc, L16c>(L, kind, prec, recon, nrhs, reps, ms)
+                     : time_stencil_t<F16Acc, F32Acc, L32f>(L, kind, prec, recon, nrhs, reps, ms);
 }
 
 int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int nrhs,

@@ -1,0 +1,56 @@
+"""Times the operator kernels alone, with CUDA events, through cvcb_time_stencil.
+
+    python -m cvc_b200.stencil_timing --kind 2 --precision single --recon 12 --nrhs 12
+
+kind 0: Q_phi_tbc on one FP64 field (all V sites); kind 1: one half-lattice
+sweep of the batched solver's stencil; kind 2: one application of its normal
+operator M^+ M (four sweeps).  The lattice and gauge field are those of the
+solver benchmark (24^3x48, ranlxd seed 11, eps 0.25) unless overridden.
+Prints one line: milliseconds per call and algorithmic GB/s.
+"""
+import argparse
+import ctypes
+
+from . import lattice as _lat
+
+_PREC = {"double": 0, "single": 1, "half": 2}
+_SPINOR = {0: 192, 1: 96, 2: 52}           # bytes per site and rhs
+_LINK = {(0, 18): 144, (1, 12): 48, (1, 18): 72, (2, 12): 24, (2, 18): 72}
+
+
+def algorithmic_bytes(kind, prec, recon, nrhs, dims):
+    T, LX, LY, LZ = dims
+    V = T * LX * LY * LZ
+    Vh = V // 2
+    if kind == 0:
+        return V * (2 * 192 + 8 * 144)      # spinor in/out + 8 links per site (FP64)
+    links = 4 * V * _LINK[(prec, 18 if prec == 0 else recon)]
+    sweep = lambda nf: nrhs * Vh * nf * _SPINOR[prec] + links
+    return sweep(2) if kind == 1 else 2 * sweep(2) + 2 * sweep(3)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--kind", type=int, default=1, choices=(0, 1, 2))
+    ap.add_argument("--precision", default="single", choices=tuple(_PREC))
+    ap.add_argument("--recon", type=int, default=12, choices=(12, 18))
+    ap.add_argument("--nrhs", type=int, default=12)
+    ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--dims", type=int, nargs=4, default=(48, 24, 24, 24), metavar=("T", "LX", "LY", "LZ"))
+    ap.add_argument("--eps", type=float, default=0.25)
+    ap.add_argument("--seed", type=int, default=11)
+    a = ap.parse_args(argv)
+    prec = _PREC[a.precision]
+    lat = _lat.Lattice(*a.dims, kappa=0.155, mu=0.005 / 0.31)
+    lat.upload_gauge(_lat.gauge_random(*a.dims, a.eps, a.seed))
+    ms = ctypes.c_double()
+    _lat._check("cvcb_time_stencil", lat._lib.cvcb_time_stencil(
+        lat._h, a.kind, prec, a.recon, a.nrhs, a.reps, ctypes.byref(ms)))
+    nbytes = algorithmic_bytes(a.kind, prec, a.recon, a.nrhs, a.dims)
+    print(f"kind {a.kind} {a.precision} recon {a.recon} nrhs {a.nrhs} dims {list(a.dims)}: "
+          f"{ms.value:.4f} ms per call, {nbytes / ms.value / 1e6:.1f} GB/s algorithmic")
+    lat.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -236,7 +236,9 @@ int cvcb_solve(cvcb_lattice *lat, double *const *x, const double *const *b, int 
  * after one warm-up launch.  kind 0: the full-lattice FP64 kernel behind
  * cvcb_Q_phi_tbc (one field, all V sites); kind 1: one half-lattice sweep of
  * the batched solver's stencil (V/2 output sites) for nrhs right-hand sides
- * in the given precision and link format, with the autotuned launch shape.
+ * in the given precision and link format, with the autotuned launch shape;
+ * kind 2: one application of the solver's normal operator M^+ M (four such
+ * sweeps), reported per application.
  * Field contents are zero (timing does not depend on them). */
 int cvcb_time_stencil(cvcb_lattice *lat, int kind, int precision, int link_recon, int nrhs,
                       int reps, double *ms_per_launch);

@@ -137,3 +137,29 @@ def test_batched_solver_zero_rhs(cb, env):
     st = lat.solve(xs, bs)
     assert st.converged == 2
     assert not np.any(xs[0])
+
+
+@pytest.mark.parametrize("prec", [1, 2], ids=["fp32", "fp16"])
+def test_batched_solver_tiny_magnitudes(cb, prec):
+    """A source scaled by 1e-33: far from it the propagator and the residuals
+    fall below the smallest normal float.  The FP16 store (one float scale
+    per site) must write such sites as zero rather than overflow 1/scale;
+    the solution is the unscaled one times 1e-33 (the solver is linear)."""
+    dims = (16, 8, 8, 8)
+    V = 16 * 8 ** 3
+    lat = cb.Lattice(*dims, kappa=0.155, mu=0.005 / 0.31)
+    lat.upload_gauge(cb.gauge_random(*dims, 0.25, 11))
+    p = cb.solver_defaults()
+    p.precision = prec
+    b1 = [point_source(V, sc) for sc in (0, 7)]
+    bt = [1e-33 * b for b in b1]
+    x1 = [np.zeros(24 * V) for _ in b1]
+    xt = [np.zeros(24 * V) for _ in bt]
+    st1 = lat.solve(x1, b1, p)
+    stt = lat.solve(xt, bt, p)
+    assert st1.converged == 2 and stt.converged == 2
+    assert stt.max_true_res <= 1e-10
+    for a, b in zip(x1, xt):
+        assert np.all(np.isfinite(b))
+        assert rel_err(1e33 * b, a) < 1e-8
+    lat.close()

@@ -102,3 +102,12 @@ def test_no_gpu_needed_for_host_api(cb):
     # geometry and generators work without touching a device
     assert cb.geometry_tables(2, 2, 2, 2)["g_iup"].size == 64
     assert cb.last_error() is not None
+
+
+def test_stencil_timing_algorithmic_bytes():
+    """Byte counts the profiles and the bench roofline use (24^3x48, 12 rhs)."""
+    from cvc_b200.stencil_timing import algorithmic_bytes
+    dims = (48, 24, 24, 24)
+    assert algorithmic_bytes(1, 1, 12, 12, dims) == 891_813_888
+    assert algorithmic_bytes(2, 1, 12, 12, dims) == 2 * 891_813_888 + 2 * 1_274_019_840
+    assert algorithmic_bytes(0, 0, 18, 1, dims) == 663_552 * (2 * 192 + 8 * 144)
