@@ -51,6 +51,7 @@ class SolverStats(ctypes.Structure):
         ("converged", _I),
         ("max_true_res", _D),
         ("seconds", _D),
+        ("batch_rhs", _I),
     ]
 
 

@@ -350,4 +350,88 @@ __global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop(HopArgs<SF, LF> A) {
   }
 }
 
+// Shared-memory staged variant, one rhs per thread, blockDim.y rhs rows per
+// block: the 8 links of each site (phased, 12-real forms rebuilt) and its 8
+// neighbour indices are produced once per block -- thread row ty builds link
+// slots ty, ty + blockDim.y, ... -- and read from shared memory by every rhs
+// row.  Link traffic from L2 and the link arithmetic per rhs fall by the
+// number of rows.  Shared memory: 8 * 9 * blockDim.x complex + 8 * blockDim.x
+// ints (slot d = 2 mu + 1 forward, 2 mu backward).
+template <typename R>
+__host__ __device__ constexpr size_t staged_smem_bytes(int bx) {
+  return (size_t)8 * 9 * bx * sizeof(Cx<R>) + (size_t)8 * bx * sizeof(int);
+}
+
+template <class SF, class LF, bool G5IN, bool G5HOP, bool AUX>
+__global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop_staged(HopArgs<SF, LF> A) {
+  using R = typename SF::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int bx = blockDim.x, tx = threadIdx.x, ty = threadIdx.y;
+  Cx<R> *sl = reinterpret_cast<Cx<R> *>(smem_raw);  // [8][9][bx]
+  int *snb = reinterpret_cast<int *>(smem_raw + (size_t)8 * 9 * bx * sizeof(Cx<R>));  // [8][bx]
+  const int r = blockIdx.x * blockDim.y + ty;
+  const bool act = r < A.nrhs && !(A.done && A.done[r]);
+  if (!__syncthreads_or(act)) return;  // uniform: no row of this block is active
+  const Geom &g = A.eg.g;
+  const int p = A.eg.p;
+  const int qoff = (1 - p) * g.Vh;
+  for (int sb = blockIdx.y; sb * bx < g.Vh; sb += gridDim.y) {
+    const int i = sb * bx + tx;
+    const bool valid = i < g.Vh;
+    if (valid) {
+      const SiteCoord cd = site_coord(g, p, i);
+      for (int d = ty; d < 8; d += blockDim.y) {
+        const int mu = d >> 1;
+        const bool fwd = d & 1;
+        const int j = nb_lex(g, cd, mu, fwd ? +1 : -1) >> 1;
+        const Link<R> W = phased_link<R>(A.links, mu, fwd ? p * g.Vh + i : qoff + j);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) sl[(d * 9 + k) * bx + tx] = W.m[k / 3][k % 3];
+        snb[d * bx + tx] = j;
+      }
+    }
+    __syncthreads();
+    if (valid && act) {
+      Spinor<R> acc;
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc.c[s][c] = cx((R)0, (R)0);
+#pragma unroll
+      for (int mu = 0; mu < 4; ++mu) {
+#pragma unroll
+        for (int fwd = 0; fwd < 2; ++fwd) {
+          const int d = 2 * mu + fwd;
+          Link<R> W;
+#pragma unroll
+          for (int k = 0; k < 9; ++k) W.m[k / 3][k % 3] = sl[(d * 9 + k) * bx + tx];
+          Spinor<R> f = A.in.load(r, snb[d * bx + tx]);
+          if (G5IN) g5_inplace(f);
+          if (fwd)  // (1 - g_mu) U_mu(x) in(x+mu)
+            accum_recon(mu, -1, acc, link_mul(W, project(mu, -1, f)));
+          else  // (1 + g_mu) U_mu(x-mu)^+ in(x-mu)
+            accum_recon(mu, +1, acc, link_dag_mul(W, project(mu, +1, f)));
+        }
+      }
+      if (G5HOP) g5_inplace(acc);
+      const R c = (R)A.c;
+      Spinor<R> o;
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) o.c[s][q] = c * acc.c[s][q];
+      o = diag_op((R)A.d1a, (R)A.d1b, o);
+      if (AUX) {
+        const Spinor<R> x = diag_op((R)A.d2a, (R)A.d2b, A.aux.load(r, i));
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+          for (int q = 0; q < 3; ++q) o.c[s][q] = o.c[s][q] + x.c[s][q];
+      }
+      A.out.store(r, i, o);
+    }
+    __syncthreads();  // the next site block overwrites the staged links
+  }
+}
+
 }  // namespace cvcb

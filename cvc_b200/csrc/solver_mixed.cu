@@ -17,6 +17,7 @@
 //   Finally x_e = A_ee^-1 (b_e + 1/2 H_eo x_o) and |b - Q x| is checked with
 //   the full-lattice FP64 operator.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -37,6 +38,7 @@ namespace cvcb {
 namespace {
 
 constexpr int kMaxBatch = 24;
+constexpr size_t kMaxStagedSmem = 200 * 1024;  // opt-in dynamic shared memory of the staged stencil
 
 // ---- batched reductions: blockIdx.y = right-hand side ----------------------
 struct BatchRed {
@@ -405,6 +407,7 @@ struct Batch {
   int n;  // rhs in this batch
   Geom g;
   LaunchShape shape;
+  LaunchShape shape64;  // FP64 sweeps when the inner iterations are sloppy
   // FP64 fields: full lattice, stride V, rhs stride 12V
   double2 *b64, *x64, *t64, *y64, *bh64;
   // sloppy fields: half lattice, compact
@@ -438,10 +441,9 @@ struct Batch {
   int hop(AF out, AF in, AF aux, LL lk, int parity, const int *done, double d1a, double d1b,
           double d2a, double d2b, double c) {
     HopArgs<AF, LL> a{out, in, aux, lk, EoGeom{g, parity}, n, done, d1a, d1b, d2a, d2b, c};
-    // FP64 sweeps of a reduced-precision solve (reliable updates) use a
-    // fixed shape; FP64 kernels keep one rhs per thread (register budget).
-    LaunchShape sh = sizeof(typename AF::R) == 8 && sizeof(typename SF::R) != 8
-                         ? LaunchShape{64, 1, 1} : shape;
+    // FP64 sweeps of a reduced-precision solve (reliable updates) have their
+    // own tuned shape; FP64 kernels keep one rhs per thread (register budget).
+    LaunchShape sh = sizeof(typename AF::R) == 8 && sizeof(typename SF::R) != 8 ? shape64 : shape;
     if (sizeof(typename AF::R) == 8) sh.nr = 1;
     const int groups = (n + sh.nr - 1) / sh.nr;
     const int by = std::min(sh.by, groups);
@@ -454,7 +456,23 @@ struct Batch {
       CVCB_CUDA(cudaEventCreate(&rec.b));
       CVCB_CUDA(cudaEventRecordWithFlags(rec.a, L->stream, capturing ? cudaEventRecordExternal : 0));
     }
-    if constexpr (sizeof(typename AF::R) == 8) {
+    if (by > 1 && sh.nr == 1) {
+      // rows of the block share links staged in shared memory
+      auto kern = k_eo_hop_staged<AF, LL, G5IN, G5HOP, AUX>;
+      const size_t smem = staged_smem_bytes<typename AF::R>(sh.bx);
+      static std::atomic<unsigned long long> attr_set{0};  // per instantiation, bit per device
+      const unsigned long long bit = 1ull << (L->device & 63);
+      if (!(attr_set.load() & bit)) {
+        CVCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kMaxStagedSmem));
+        attr_set.fetch_or(bit);
+      }
+      if (smem > kMaxStagedSmem) {
+        set_error("staged stencil: %zu bytes of shared memory", smem);
+        return CVCB_ERR_ARG;
+      }
+      kern<<<grid, block, smem, L->stream>>>(a);
+    } else if constexpr (sizeof(typename AF::R) == 8) {
       k_eo_hop<AF, LL, 1, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
     } else {
       switch (sh.nr) {
@@ -713,7 +731,11 @@ int time_ms(cvcb_lattice *L, Fn fn, int reps, float *best) {
 // Autotuner for the stencil launch shape: sites per block x right-hand sides
 // per block, timed on the sloppy normal operator.
 template <class SF, class XF, class LF>
-int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon) {
+int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int block_threads = 0) {
+  if (block_threads > 0) {  // caller's choice: that many sites per block, one rhs per thread
+    B.shape = LaunchShape{block_threads, 1, 1};
+    return CVCB_OK;
+  }
   auto key = std::make_tuple(L->g.V, prec, recon, B.n);
   auto it = g_tuned_shape.find(key);
   if (it != g_tuned_shape.end()) {
@@ -735,7 +757,7 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon) {
   LaunchShape best;
   float best_ms = 1e30f;
   const int bxs[] = {32, 64, 128, 256};
-  const int bys[] = {1, 2, 4};
+  const int bys[] = {1, 2, 3, 4, 6};
   const int nrs[] = {1, 2, 3, 4};
   const bool fp64 = sizeof(typename SF::R) == 8;
   for (int nr : nrs)
@@ -761,6 +783,37 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon) {
   return CVCB_OK;
 }
 
+// Shape of the FP64 sweeps of the reliable updates in a reduced-precision
+// solve, timed on M(mu) in FP64 (two sweeps).
+template <class SF, class XF, class LF>
+int tune_shape64(cvcb_lattice *L, Batch<SF, XF, LF> &B) {
+  auto key = std::make_tuple(L->g.V, -1, 18, B.n);
+  auto it = g_tuned_shape.find(key);
+  if (it != g_tuned_shape.end()) {
+    B.shape64 = it->second;
+    return CVCB_OK;
+  }
+  const LaunchShape cands[] = {{64, 1, 1}, {128, 1, 1}, {32, 2, 1}, {64, 2, 1}, {32, 3, 1},
+                               {32, 4, 1}, {16, 4, 1}, {64, 3, 1}, {32, 6, 1}, {16, 6, 1}};
+  LaunchShape best{64, 1, 1};
+  float best_ms = 1e30f;
+  for (const LaunchShape &c : cands) {
+    B.shape64 = c;
+    float ms;
+    if (time_ms(L, [&] { return B.schur64(B.y64, B.x64, B.mu, nullptr); }, 3, &ms) != CVCB_OK) {
+      cudaGetLastError();
+      continue;
+    }
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  B.shape64 = best;
+  g_tuned_shape[key] = best;
+  return CVCB_OK;
+}
+
 template <class SF, class XF, class LF>
 int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
               const cvcb_solver_params *P, cvcb_solver_stats *st, LaunchShape *shape_out) {
@@ -773,7 +826,8 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   dim3 rg(red_blocks_sites(g.Vh), n), rgf(red_blocks_sites(g.V), n);
 
   for (int i = 0; i < n; ++i) CVCB_TRY(spinor_in(L, B.b64 + i * fs, b[i], g.V));
-  CVCB_TRY(tune_shape(L, B, P->precision, P->link_recon));
+  CVCB_TRY(tune_shape(L, B, P->precision, P->link_recon, P->block_threads));
+  if (sizeof(typename SF::R) != 8) CVCB_TRY(tune_shape64(L, B));
   if (shape_out) *shape_out = B.shape;
 
   // |b|^2 over the full lattice
@@ -816,8 +870,11 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   CVCB_CUDA(cudaMemcpyAsync(B.S.done, done.data(), n * sizeof(int), cudaMemcpyHostToDevice,
                             L->stream));
 
-  // capture a chunk of iterations in a CUDA graph
-  const int chunk = 10;
+  // One CG iteration is captured in a CUDA graph; between two host checks the
+  // graph is launched k times, k <= kmax, with k cut to the number of
+  // iterations each rhs is predicted to need (from its measured convergence
+  // rate) so that the last chunk does not overshoot convergence.
+  const int kmax = 10;
   cudaGraphExec_t gexec = nullptr;
   long long graph_nodes = 0;
   if (P->use_graph) {
@@ -825,11 +882,8 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     const long long before = L->nlaunch;
     CVCB_CUDA(cudaStreamBeginCapture(L->stream, cudaStreamCaptureModeThreadLocal));
     B.capturing = true;
-    int rc = CVCB_OK;
-    for (int k = 0; k < chunk && rc == CVCB_OK; ++k) {
-      B.prof_rec = L->prof && k == 0;
-      rc = B.iteration();
-    }
+    B.prof_rec = L->prof;
+    int rc = B.iteration();
     B.prof_rec = false;
     B.capturing = false;
     cudaError_t ec = cudaStreamEndCapture(L->stream, &graph);
@@ -859,8 +913,16 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     return CVCB_OK;
   };
 
-  const double delta2 = P->delta * P->delta;
+  // delta 0: by the storage of the inner iterations -- an FP16 recursion
+  // drifts from the true residual after about three decades, FP32 after six
+  const double delta = P->delta > 0 ? P->delta
+                       : std::is_same<SF, F16Acc>::value ? 0.1
+                       : std::is_same<SF, F32Acc>::value ? 1e-4 : 1e-8;
+  const double delta2 = delta * delta;
   int total_iter = 0, nru = 0, nrestart = 0;
+  // rr at the previous check (same units) and the measured per-iteration
+  // factor of rr (0 = not known yet)
+  std::vector<double> rr_ref(rr), rate(n, 0.0);
   const double t0 = now_s();
   int rc = CVCB_OK;
   while (true) {
@@ -870,14 +932,22 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     if (total_iter >= P->max_iter) break;
     int active = 0;
     for (int i = 0; i < n; ++i) active += !done[i];
+    int chunk = std::min(kmax, P->max_iter - total_iter);
+    for (int i = 0; i < n; ++i) {
+      if (done[i] || !(rate[i] > 0 && rate[i] < 1) || !(rr[i] > 0)) continue;
+      const double need = std::log(target2[i] * ratio2[i] / rr[i]) / std::log(rate[i]);
+      if (std::isfinite(need)) chunk = std::min(chunk, std::max(1, (int)std::ceil(need)));
+    }
     if (gexec) {
-      cudaError_t e = cudaGraphLaunch(gexec, L->stream);
-      if (e != cudaSuccess) {
-        set_error("graph launch: %s", cudaGetErrorString(e));
-        rc = CVCB_ERR_CUDA;
-        break;
+      for (int k = 0; k < chunk && rc == CVCB_OK; ++k) {
+        cudaError_t e = cudaGraphLaunch(gexec, L->stream);
+        if (e != cudaSuccess) {
+          set_error("graph launch: %s", cudaGetErrorString(e));
+          rc = CVCB_ERR_CUDA;
+        }
+        L->nlaunch += graph_nodes;
       }
-      L->nlaunch += graph_nodes;
+      if (rc != CVCB_OK) break;
     } else {
       for (int k = 0; k < chunk; ++k) {
         B.prof_rec = L->prof && k == 0;
@@ -897,6 +967,9 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
       if (done[i]) continue;
       iters[i] += chunk;
       since[i] += chunk;
+      if (std::isfinite(rr[i]) && rr[i] > 0 && rr_ref[i] > 0 && rr[i] < rr_ref[i])
+        rate[i] = std::pow(rr[i] / rr_ref[i], 1.0 / chunk);
+      rr_ref[i] = rr[i];
       const bool bad = !std::isfinite(rr[i]);
       const bool dropped = rr[i] < delta2 * rr_max[i];
       const bool near = rr[i] / ratio2[i] < target2[i];
@@ -944,6 +1017,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
       if (skip[i]) continue;
       since[i] = 0;
       rr_max[i] = rr[i];
+      rr_ref[i] = rr[i];
       if (rhat2[i] > 0) ratio2[i] = rr[i] / rhat2[i];
       if (rhat2[i] <= target2[i]) done[i] = 1;
     }
@@ -1063,6 +1137,37 @@ int time_stencil(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int r
                      : time_stencil_t<F16Acc, F32Acc, L32f>(L, kind, prec, recon, nrhs, reps, ms);
 }
 
+// Autotuner for the number of right-hand sides per batch: the sloppy normal
+// operator is timed (with its own tuned launch shape) for each candidate
+// batch size n, and the n with the least predicted time for all nrhs,
+// ceil(nrhs / n) * t(n), wins.  Larger batches share each link load among
+// more right-hand sides but hold more registers and device memory.
+template <class SF, class XF, class LF>
+int tune_batch(cvcb_lattice *L, const cvcb_solver_params *P, int recon, int nrhs, int *nb_out) {
+  const int cands[] = {4, 6, 8, 12, 16, 24};
+  double best_t = 1e300;
+  int best = std::min(nrhs, 12);
+  for (int n : cands) {
+    if (n > kMaxBatch || (n > nrhs && n != cands[0])) continue;
+    Batch<SF, XF, LF> B;
+    CVCB_TRY(setup_batch(L, B, n, /*with_fp64=*/false));
+    CVCB_CUDA(cudaMemsetAsync(B.p.p, 0, sloppy_site_bytes<SF>() * (size_t)L->g.Vh * n, L->stream));
+    CVCB_TRY(tune_shape(L, B, P->precision, recon, P->block_threads));
+    float ms;
+    if (time_ms(L, [&] { return B.normal_op_sloppy(B.Ap, B.p, nullptr); }, 3, &ms) != CVCB_OK) {
+      cudaGetLastError();
+      continue;
+    }
+    const double t = (double)((nrhs + n - 1) / n) * ms;
+    if (t < best_t * 0.98) {  // prefer the smaller batch unless clearly slower
+      best_t = t;
+      best = std::min(n, nrhs);
+    }
+  }
+  *nb_out = best;
+  return CVCB_OK;
+}
+
 int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int nrhs,
                   const cvcb_solver_params *P, cvcb_solver_stats *st) {
   if (!L->have_gauge) {
@@ -1071,20 +1176,36 @@ int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int
   }
   if (nrhs <= 0) return CVCB_OK;
   if (P->precision < 0 || P->precision > 2 || (P->link_recon != 12 && P->link_recon != 18) ||
-      !(P->tol > 0) || !(P->delta > 0 && P->delta < 1) || P->max_iter <= 0 ||
-      P->block_rhs < 0 || P->block_rhs > kMaxBatch) {
+      !(P->tol > 0) || !(P->delta >= 0 && P->delta < 1) || P->max_iter <= 0 ||
+      P->block_rhs < 0 || P->block_rhs > kMaxBatch || P->block_threads < 0 ||
+      P->block_threads > kHopMaxThreads || P->block_threads % 32 != 0) {
     set_error("invalid solver parameters");
     return CVCB_ERR_ARG;
   }
   int recon = P->link_recon;
   if (recon == 12 && !(L->unitarity >= 0 && L->unitarity < 1e-6)) recon = 18;  // not SU(3)
   std::memset(st, 0, sizeof *st);
-  int nb = P->block_rhs ? P->block_rhs : std::min(nrhs, 12);
-  if (!P->block_rhs) {
+  int nb = P->block_rhs;
+  if (!nb) {
     auto key = std::make_tuple(L->g.V, P->precision, recon, nrhs);
     auto it = g_tuned_batch.find(key);
-    if (it != g_tuned_batch.end()) nb = it->second;
+    if (it != g_tuned_batch.end()) {
+      nb = it->second;
+    } else {
+      int rc;
+      if (P->precision == CVCB_PREC_DOUBLE)
+        rc = tune_batch<F64Acc, F64Acc, L64>(L, P, recon, nrhs, &nb);
+      else if (P->precision == CVCB_PREC_SINGLE)
+        rc = recon == 12 ? tune_batch<F32Acc, F32Acc, L32c>(L, P, recon, nrhs, &nb)
+                         : tune_batch<F32Acc, F32Acc, L32f>(L, P, recon, nrhs, &nb);
+      else
+        rc = recon == 12 ? tune_batch<F16Acc, F32Acc, L16c>(L, P, recon, nrhs, &nb)
+                         : tune_batch<F16Acc, F32Acc, L32f>(L, P, recon, nrhs, &nb);
+      if (rc < 0) return rc;
+      g_tuned_batch[key] = nb;
+    }
   }
+  st->batch_rhs = nb;
   for (int off = 0; off < nrhs; off += nb) {
     const int n = std::min(nb, nrhs - off);
     int rc;
@@ -1114,7 +1235,7 @@ void cvcb_solver_defaults(cvcb_solver_params *p) {
   p->max_iter = 20000;
   p->use_graph = 1;
   p->tol = 1e-10;
-  p->delta = 0.1;
+  p->delta = 0.0;
 }
 
 int cvcb_profile(cvcb_lattice *L, int enable) {

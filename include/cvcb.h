@@ -206,24 +206,28 @@ typedef struct {
   int precision;     /* CVCB_PREC_*: arithmetic/storage of the inner iterations */
   int link_recon;    /* 18 or 12 reals per link in the inner operator */
   int block_rhs;     /* right-hand sides per launch (0 = autotuned) */
-  int block_threads; /* threads per block in the stencil (0 = autotuned) */
+  int block_threads; /* sites per stencil block, one rhs per thread; a multiple
+                        of 32 up to 256 (0 = autotuned shape) */
   int max_iter;      /* per right-hand side */
   int use_graph;     /* capture the inner iterations in a CUDA graph */
   double tol;        /* target |b - Q x|_2 / |b|_2, checked in FP64 */
-  double delta;      /* reliable-update trigger: sloppy |r| fell by this factor */
+  double delta;      /* reliable-update trigger: sloppy |r| fell by this factor
+                        (0 = by inner precision: 0.1 FP16, 1e-4 FP32, 1e-8 FP64) */
 } cvcb_solver_params;
 
 typedef struct {
   int iterations;        /* inner iterations, summed over right-hand sides */
   int reliable_updates;  /* FP64 residual recomputations */
-  int restarts;          /* tightening restarts after the final FP64 check */
+  int restarts;          /* directions restarted from the residual (after a
+                            non-finite sloppy residual) */
   int converged;         /* right-hand sides that met tol */
   double max_true_res;   /* max over rhs of |b - Q x| / |b| in FP64 */
-  double seconds;        /* device time of the solve */
+  double seconds;        /* wall time of the iterations */
+  int batch_rhs;         /* right-hand sides per batch (given or autotuned) */
 } cvcb_solver_stats;
 
 /* Fills the defaults: single precision, 12-real links, autotuned blocks,
- * tol 1e-10, delta 0.1, max_iter 20000, graphs on. */
+ * tol 1e-10, delta 0 (by precision), max_iter 20000, graphs on. */
 void cvcb_solver_defaults(cvcb_solver_params *p);
 
 /* x[i], b[i] for i < nrhs: CVC-layout spinor fields (host or device).  x is
