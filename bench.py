@@ -252,7 +252,7 @@ def main():
     n0 = ctypes.c_longlong()
     lat._lib.cvcb_counters(lat._h, ctypes.byref(n0), None, None, None)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    worst_res, iters = 0.0, 0
+    worst_res, iters, nb = 0.0, 0, 12
     with Clocks(local) as clk:
         e0.record(stream)
         t0 = time.perf_counter()
@@ -260,6 +260,7 @@ def main():
             st = step()
             worst_res = max(worst_res, st.max_true_res)
             iters += st.iterations
+            nb = st.batch_rhs
         e1.record(stream)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
@@ -286,10 +287,8 @@ def main():
     stencil_avg_ms = pms.value / max(pl.value, 1)
     stencil_bytes = pbytes.value / max(pl.value, 1)
     achieved = stencil_bytes / (stencil_avg_ms * 1e-3) / 1e9 if pl.value else None
-    shape_bx, shape_by = ctypes.c_int(), ctypes.c_int()
-    nb = 12
-    lat._lib.cvcb_tuned_shape(lat._h, prec, params.link_recon, nb, ctypes.byref(shape_bx),
-                              ctypes.byref(shape_by))
+    shape = [ctypes.c_int() for _ in range(4)]
+    lat._lib.cvcb_tuned_shape(lat._h, prec, params.link_recon, nb, *[ctypes.byref(v) for v in shape])
     traffic_key = f"{args.precision}-{params.link_recon}-n{nb}-{T}x{LX}x{LY}x{LZ}"
     traffic = stencil_traffic_from_profile(traffic_key)
 
@@ -307,7 +306,11 @@ def main():
             f"{args.precision} inner iterations, FP64 reliable updates, batched",
             "link_recon": params.link_recon, "parallelism": f"rhs-sharded x{world}",
             "l2": "inputs larger than L2 (96 x 127 MB fields)",
-            "stencil_shape": [shape_bx.value, shape_by.value],
+            "rhs_per_batch": nb,
+            "stencil_shape": {"sites_per_block": shape[0].value, "rows_per_block": shape[1].value,
+                              "rhs_per_thread": shape[2].value,
+                              "variant": ["per-thread links", "shared-memory links",
+                                          "packed FP32x2 rhs pairs"][shape[3].value]},
             "inner_iterations_per_step": iters // max(args.steps, 1),
             "max_true_residual": worst_res,
         },

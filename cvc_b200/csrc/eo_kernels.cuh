@@ -350,6 +350,212 @@ __global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop(HopArgs<SF, LF> A) {
   }
 }
 
+// ---- two right-hand sides per thread in packed FP32x2 arithmetic -----------
+// Lane x of every float2 belongs to rhs a, lane y to rhs b.  The link is the
+// same for both, so each complex multiply-add of the link product is two
+// packed FMAs (one instruction per two rhs); the link rebuild, the neighbour
+// indices and the addresses are shared by the pair as well.
+struct CP {  // complex pair: re = (a.re, b.re), im = (a.im, b.im)
+  float2 re, im;
+};
+__device__ __forceinline__ float2 bc(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 neg2(float2 v) { return make_float2(-v.x, -v.y); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, neg2(b)); }
+
+struct HalfPair {
+  CP c[2][3];
+};
+struct SpinorPair {
+  CP c[4][3];
+};
+
+__device__ __forceinline__ HalfPair pair_half(const HalfSpinor<float> &a, const HalfSpinor<float> &b) {
+  HalfPair h;
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      h.c[s][c].re = make_float2(a.c[s][c].re, b.c[s][c].re);
+      h.c[s][c].im = make_float2(a.c[s][c].im, b.c[s][c].im);
+    }
+  return h;
+}
+
+// u = W h (dag = false) or W^+ h (dag = true), both rhs at once
+template <bool DAG>
+__device__ __forceinline__ HalfPair link_mul_pair(const Link<float> &W, const HalfPair &h) {
+  HalfPair u;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    // row i of W (or of W^+): w_j = W[i][j] or conj(W[j][i])
+    float wr[3], wi[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      wr[j] = DAG ? W.m[j][i].re : W.m[i][j].re;
+      wi[j] = DAG ? -W.m[j][i].im : W.m[i][j].im;
+    }
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      float2 re = __fmul2_rn(bc(wr[0]), h.c[s][0].re);
+      float2 im = __fmul2_rn(bc(wr[0]), h.c[s][0].im);
+      re = __ffma2_rn(bc(-wi[0]), h.c[s][0].im, re);
+      im = __ffma2_rn(bc(wi[0]), h.c[s][0].re, im);
+#pragma unroll
+      for (int j = 1; j < 3; ++j) {
+        re = __ffma2_rn(bc(wr[j]), h.c[s][j].re, re);
+        im = __ffma2_rn(bc(wr[j]), h.c[s][j].im, im);
+        re = __ffma2_rn(bc(-wi[j]), h.c[s][j].im, re);
+        im = __ffma2_rn(bc(wi[j]), h.c[s][j].re, im);
+      }
+      u.c[s][i].re = re;
+      u.c[s][i].im = im;
+    }
+  }
+  return u;
+}
+
+// acc += (1 + s g_mu)-reconstruction of u, both rhs (see accum_recon)
+__device__ __forceinline__ void accum_recon_pair(int mu, int s, SpinorPair &acc, const HalfPair &u) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    acc.c[0][c].re = add2(acc.c[0][c].re, u.c[0][c].re);
+    acc.c[0][c].im = add2(acc.c[0][c].im, u.c[0][c].im);
+    acc.c[1][c].re = add2(acc.c[1][c].re, u.c[1][c].re);
+    acc.c[1][c].im = add2(acc.c[1][c].im, u.c[1][c].im);
+    // spins 2, 3: +-u or +-i u of spins 0, 1; i (x + i y) = -y + i x
+    switch (mu) {
+      case 0:  // r2 = -s u0, r3 = -s u1
+        if (s > 0) {
+          acc.c[2][c].re = sub2(acc.c[2][c].re, u.c[0][c].re);
+          acc.c[2][c].im = sub2(acc.c[2][c].im, u.c[0][c].im);
+          acc.c[3][c].re = sub2(acc.c[3][c].re, u.c[1][c].re);
+          acc.c[3][c].im = sub2(acc.c[3][c].im, u.c[1][c].im);
+        } else {
+          acc.c[2][c].re = add2(acc.c[2][c].re, u.c[0][c].re);
+          acc.c[2][c].im = add2(acc.c[2][c].im, u.c[0][c].im);
+          acc.c[3][c].re = add2(acc.c[3][c].re, u.c[1][c].re);
+          acc.c[3][c].im = add2(acc.c[3][c].im, u.c[1][c].im);
+        }
+        break;
+      case 1:  // r2 = s i u1, r3 = s i u0
+        if (s > 0) {
+          acc.c[2][c].re = sub2(acc.c[2][c].re, u.c[1][c].im);
+          acc.c[2][c].im = add2(acc.c[2][c].im, u.c[1][c].re);
+          acc.c[3][c].re = sub2(acc.c[3][c].re, u.c[0][c].im);
+          acc.c[3][c].im = add2(acc.c[3][c].im, u.c[0][c].re);
+        } else {
+          acc.c[2][c].re = add2(acc.c[2][c].re, u.c[1][c].im);
+          acc.c[2][c].im = sub2(acc.c[2][c].im, u.c[1][c].re);
+          acc.c[3][c].re = add2(acc.c[3][c].re, u.c[0][c].im);
+          acc.c[3][c].im = sub2(acc.c[3][c].im, u.c[0][c].re);
+        }
+        break;
+      case 2:  // r2 = s u1, r3 = -s u0
+        if (s > 0) {
+          acc.c[2][c].re = add2(acc.c[2][c].re, u.c[1][c].re);
+          acc.c[2][c].im = add2(acc.c[2][c].im, u.c[1][c].im);
+          acc.c[3][c].re = sub2(acc.c[3][c].re, u.c[0][c].re);
+          acc.c[3][c].im = sub2(acc.c[3][c].im, u.c[0][c].im);
+        } else {
+          acc.c[2][c].re = sub2(acc.c[2][c].re, u.c[1][c].re);
+          acc.c[2][c].im = sub2(acc.c[2][c].im, u.c[1][c].im);
+          acc.c[3][c].re = add2(acc.c[3][c].re, u.c[0][c].re);
+          acc.c[3][c].im = add2(acc.c[3][c].im, u.c[0][c].im);
+        }
+        break;
+      default:  // r2 = s i u0, r3 = -s i u1
+        if (s > 0) {
+          acc.c[2][c].re = sub2(acc.c[2][c].re, u.c[0][c].im);
+          acc.c[2][c].im = add2(acc.c[2][c].im, u.c[0][c].re);
+          acc.c[3][c].re = add2(acc.c[3][c].re, u.c[1][c].im);
+          acc.c[3][c].im = sub2(acc.c[3][c].im, u.c[1][c].re);
+        } else {
+          acc.c[2][c].re = add2(acc.c[2][c].re, u.c[0][c].im);
+          acc.c[2][c].im = sub2(acc.c[2][c].im, u.c[0][c].re);
+          acc.c[3][c].re = sub2(acc.c[3][c].re, u.c[1][c].im);
+          acc.c[3][c].im = add2(acc.c[3][c].im, u.c[1][c].re);
+        }
+        break;
+    }
+  }
+}
+
+// Packed-pair stencil: thread = (site, rhs pair); same sweep as k_eo_hop.
+template <class SF, class LF, bool G5IN, bool G5HOP, bool AUX>
+__global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop_x2(HopArgs<SF, LF> A) {
+  static_assert(sizeof(typename SF::R) == 4, "packed pairs need FP32 arithmetic");
+  const int ra = (blockIdx.x * blockDim.y + threadIdx.y) * 2;
+  if (ra >= A.nrhs) return;
+  const bool act_a = !(A.done && A.done[ra]);
+  const bool has_b = ra + 1 < A.nrhs;
+  const bool act_b = has_b && !(A.done && A.done[ra + 1]);
+  if (!act_a && !act_b) return;
+  const int rb = has_b ? ra + 1 : ra;  // a lone last rhs runs twice, stores once
+  const Geom &g = A.eg.g;
+  const int p = A.eg.p;
+  const int qoff = (1 - p) * g.Vh;
+  for (int sb = blockIdx.y; sb * (int)blockDim.x < g.Vh; sb += gridDim.y) {
+    const int i = sb * blockDim.x + threadIdx.x;
+    if (i >= g.Vh) return;
+    const SiteCoord cd = site_coord(g, p, i);
+    SpinorPair acc;
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc.c[s][c].re = acc.c[s][c].im = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+      {  // backward: (1 + g_mu) U_mu(x-mu)^+ in(x-mu)
+        const int j = nb_lex(g, cd, mu, -1) >> 1;
+        const Link<float> W = phased_link<float>(A.links, mu, qoff + j);
+        Spinor<float> fa = A.in.load(ra, j), fb = A.in.load(rb, j);
+        if (G5IN) {
+          g5_inplace(fa);
+          g5_inplace(fb);
+        }
+        const HalfPair h = pair_half(project(mu, +1, fa), project(mu, +1, fb));
+        accum_recon_pair(mu, +1, acc, link_mul_pair<true>(W, h));
+      }
+      {  // forward: (1 - g_mu) U_mu(x) in(x+mu)
+        const int j = nb_lex(g, cd, mu, +1) >> 1;
+        const Link<float> W = phased_link<float>(A.links, mu, p * g.Vh + i);
+        Spinor<float> fa = A.in.load(ra, j), fb = A.in.load(rb, j);
+        if (G5IN) {
+          g5_inplace(fa);
+          g5_inplace(fb);
+        }
+        const HalfPair h = pair_half(project(mu, -1, fa), project(mu, -1, fb));
+        accum_recon_pair(mu, -1, acc, link_mul_pair<false>(W, h));
+      }
+    }
+    const float c = (float)A.c;
+#pragma unroll
+    for (int lane = 0; lane < 2; ++lane) {
+      if (lane == 0 ? !act_a : !act_b) continue;
+      const int r = lane == 0 ? ra : rb;
+      Spinor<float> o;
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const CP v = acc.c[s][q];
+          o.c[s][q] = lane == 0 ? cx(c * v.re.x, c * v.im.x) : cx(c * v.re.y, c * v.im.y);
+        }
+      if (G5HOP) g5_inplace(o);
+      o = diag_op((float)A.d1a, (float)A.d1b, o);
+      if (AUX) {
+        const Spinor<float> x = diag_op((float)A.d2a, (float)A.d2b, A.aux.load(r, i));
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+          for (int q = 0; q < 3; ++q) o.c[s][q] = o.c[s][q] + x.c[s][q];
+      }
+      A.out.store(r, i, o);
+    }
+  }
+}
+
 // Shared-memory staged variant, one rhs per thread, blockDim.y rhs rows per
 // block: the 8 links of each site (phased, 12-real forms rebuilt) and its 8
 // neighbour indices are produced once per block -- thread row ty builds link

@@ -374,6 +374,7 @@ struct RedResid {
 // ---------------------------------------------------------------------------
 struct LaunchShape {
   int bx = 64, by = 1, nr = 1;  // sites per block, rhs groups per block, rhs per thread
+  int pk = 0;                   // 1: nr == 2 in packed FP32x2 arithmetic (k_eo_hop_x2)
 };
 
 // Autotuner results, per process: (V, precision, recon, n) -> launch shape,
@@ -456,7 +457,15 @@ struct Batch {
       CVCB_CUDA(cudaEventCreate(&rec.b));
       CVCB_CUDA(cudaEventRecordWithFlags(rec.a, L->stream, capturing ? cudaEventRecordExternal : 0));
     }
-    if (by > 1 && sh.nr == 1) {
+    bool packed = false;
+    if constexpr (sizeof(typename AF::R) == 4) {
+      if (sh.pk) {  // two rhs per thread in packed FP32x2 arithmetic
+        k_eo_hop_x2<AF, LL, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
+        packed = true;
+      }
+    }
+    if (packed) {
+    } else if (by > 1 && sh.nr == 1) {
       // rows of the block share links staged in shared memory
       auto kern = k_eo_hop_staged<AF, LL, G5IN, G5HOP, AUX>;
       const size_t smem = staged_smem_bytes<typename AF::R>(sh.bx);
@@ -742,13 +751,15 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
     B.shape = it->second;
     return CVCB_OK;
   }
-  // CVCB_SHAPE="sites,rows,rhs_per_thread" pins the shape (reproducible runs,
-  // profiling); otherwise every admissible shape is timed.
+  // CVCB_SHAPE="sites,rows,rhs_per_thread[,packed]" pins the shape
+  // (reproducible runs, profiling); otherwise every admissible shape is timed.
   if (const char *env = getenv("CVCB_SHAPE")) {
     LaunchShape f;
-    if (sscanf(env, "%d,%d,%d", &f.bx, &f.by, &f.nr) == 3 && f.bx > 0 && f.by > 0 && f.nr >= 1 &&
-        f.nr <= 4 && f.bx * f.by <= kHopMaxThreads) {
-      if (sizeof(typename SF::R) == 8) f.nr = 1;
+    const int nf = sscanf(env, "%d,%d,%d,%d", &f.bx, &f.by, &f.nr, &f.pk);
+    if (nf >= 3 && f.bx > 0 && f.by > 0 && f.nr >= 1 && f.nr <= 4 &&
+        f.bx * f.by <= kHopMaxThreads) {
+      if (nf < 4 || f.nr != 2) f.pk = 0;
+      if (sizeof(typename SF::R) == 8) f.nr = 1, f.pk = 0;
       B.shape = f;
       g_tuned_shape[key] = f;
       return CVCB_OK;
@@ -758,16 +769,20 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
   float best_ms = 1e30f;
   const int bxs[] = {32, 64, 128, 256};
   const int bys[] = {1, 2, 3, 4, 6};
-  const int nrs[] = {1, 2, 3, 4};
+  // (rhs per thread, packed): 2 rhs per thread either as two unpacked
+  // spinors or as FP32x2 pairs
+  const int nrs[][2] = {{1, 0}, {2, 0}, {3, 0}, {4, 0}, {2, 1}};
   const bool fp64 = sizeof(typename SF::R) == 8;
-  for (int nr : nrs)
+  for (const auto &np : nrs)
     for (int bx : bxs)
     for (int by : bys) {
+      const int nr = np[0];
       if (fp64 && nr > 1) continue;
       if (nr > B.n || by * nr > B.n || bx * by > kHopMaxThreads || bx * by < 32) continue;
       B.shape.bx = bx;
       B.shape.by = by;
       B.shape.nr = nr;
+      B.shape.pk = np[1];
       float ms;
       if (time_ms(L, [&] { return B.normal_op_sloppy(B.Ap, B.p, nullptr); }, 3, &ms) != CVCB_OK) {
         cudaGetLastError();
@@ -1260,16 +1275,19 @@ int cvcb_counters(cvcb_lattice *L, long long *kernel_launches, long long *stenci
 }
 
 int cvcb_tuned_shape(cvcb_lattice *L, int precision, int link_recon, int nrhs, int *sites_per_block,
-                     int *rhs_per_block) {
-  if (!L || !sites_per_block || !rhs_per_block) return CVCB_ERR_NULL;
-  // rhs_per_block = rhs groups per block x rhs per thread
+                     int *rows_per_block, int *rhs_per_thread, int *variant) {
+  if (!L || !sites_per_block || !rows_per_block || !rhs_per_thread || !variant)
+    return CVCB_ERR_NULL;
   auto it = cvcb::g_tuned_shape.find(std::make_tuple(L->g.V, precision, link_recon, nrhs));
   if (it == cvcb::g_tuned_shape.end()) {
     cvcb::set_error("no tuned shape for this configuration yet");
     return CVCB_ERR_STATE;
   }
-  *sites_per_block = it->second.bx;
-  *rhs_per_block = it->second.by * 100 + it->second.nr;
+  const cvcb::LaunchShape &s = it->second;
+  *sites_per_block = s.bx;
+  *rows_per_block = s.by;
+  *rhs_per_thread = s.nr;
+  *variant = s.pk ? 2 : (s.by > 1 && s.nr == 1) ? 1 : 0;
   return CVCB_OK;
 }
 

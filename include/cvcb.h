@@ -248,11 +248,14 @@ int cvcb_time_stencil(cvcb_lattice *lat, int kind, int precision, int link_recon
                       int reps, double *ms_per_launch);
 
 /* Launch shape the autotuner chose for the batched stencil for this lattice
- * volume, precision, link format and batch size: sites per thread block, and
- * rhs_per_block = 100 * (thread rows per block) + (right-hand sides per
- * thread); CVCB_ERR_STATE before the first tuning. */
+ * volume, precision, link format and batch size: sites per thread block,
+ * thread rows per block (each row a group of right-hand sides), right-hand
+ * sides per thread, and the kernel variant (0: links per thread, 1: links
+ * staged in shared memory for all rows, 2: two rhs per thread in packed
+ * FP32x2 arithmetic); CVCB_ERR_STATE before the first tuning. */
 int cvcb_tuned_shape(cvcb_lattice *lat, int precision, int link_recon, int nrhs,
-                     int *sites_per_block, int *rhs_per_block);
+                     int *sites_per_block, int *rows_per_block, int *rhs_per_thread,
+                     int *variant);
 
 /* Instrumentation.  cvcb_profile(lat, 1) resets and starts timing the
  * batched solver's stencil: inside cvcb_solve, the stencil launches of one

@@ -114,3 +114,91 @@ def test_autograd_wrapper_and_recompute(setup, cb):
     assert abs(mu.grad.item() - dmu) <= 1e-9 * abs(dmu)
     assert abs(ka.grad.item() - dka) <= 1e-9 * abs(dka)
     assert np.allclose(gt.grad.numpy(), gu, rtol=1e-8, atol=1e-12 * np.max(np.abs(gu)))
+
+
+def test_tangent_mu_vs_reference_rerun(setup, oracle_mod):
+    """dPi/dmu against the reference rerun at mu +- h: the 120 columns are
+    solved by the reference's own invert_Qtm_her (compiled from its sources)
+    at shifted mu, contracted by the oracle contraction (bit-exact with the
+    reference's), and differenced."""
+    import oracle_bind
+    if not oracle_bind.reference_available():
+        pytest.skip("reference library not built")
+    lat, g, p = setup
+    T, LX, LY, LZ = DIMS
+    t, r = divmod(SRC, LX * LY * LZ)
+    x, r = divmod(r, LY * LZ)
+    y, z = divmod(r, LZ)
+    c = [t, x, y, z]
+    L = [T, LX, LY, LZ]
+    shifted = []
+    for m in range(4):
+        cc = list(c)
+        cc[m] = (cc[m] + 1) % L[m]
+        shifted.append(((cc[0] * LX + cc[1]) * LY + cc[2]) * LZ + cc[3])
+    shifted.append(SRC)
+    bs = []
+    for s in shifted:
+        for sc in range(12):
+            b = np.zeros(24 * V)
+            b[24 * s + 2 * sc] = 1.0
+            bs.append(b)
+    ref = oracle_bind.Reference(*DIMS, KAPPA, MU)
+    ref.set_gauge(g)
+    orc = oracle_mod.Oracle(*DIMS, KAPPA, MU)
+    orc.set_gauge(g)
+
+    def ref_pi(mu):
+        cols = []
+        for sgn in (+1, -1):
+            ref.set_params(KAPPA, sgn * mu)
+            for b in bs:
+                rc, xs = ref.invert(b, 1e-26, 5000, her=True)
+                assert rc > 0
+                cols.append(xs)
+        conn, _ = orc.cvc_contract(cols, SRC)
+        return conn
+
+    fd = (ref_pi(MU + H) - ref_pi(MU - H)) / (2 * H)
+    forward(lat, g, p)
+    d = lat.pi_tangent("mu")
+    assert np.linalg.norm(d - fd) / np.linalg.norm(fd) < 1e-6
+
+
+def test_c4_gradients_12c24(cb):
+    """The adjoint check at 12^3x24 (gauge eps 0.3 seed 3, kappa 0.150,
+    2 kappa mu 0.01, source at the origin): dPi/dmu, dPi/dkappa and dL/dU
+    (along a random direction) against central differences, h = 1e-5;
+    the relative errors are printed with -s."""
+    dims = (24, 12, 12, 12)
+    vol = 24 * 12 ** 3
+    lat = cb.Lattice(*dims, kappa=KAPPA, mu=MU)
+    g = cb.gauge_random(*dims, 0.3, 3)
+    p = cb.solver_defaults()
+    p.precision, p.link_recon, p.tol = cb.PREC_DOUBLE, 18, 1e-13
+    w = np.zeros(32 * vol)
+    w[0::32] = np.cos(2 * np.pi * (np.arange(vol) % 12) / 12)
+
+    def fwd(kappa=KAPPA, mu=MU, gg=g):
+        lat.set_params(kappa, mu)
+        lat.upload_gauge(gg)
+        return lat.pi_forward(0, p)[0]
+
+    fwd()
+    dmu_t, dka_t = lat.pi_tangent("mu"), lat.pi_tangent("kappa")
+    dmu, dka, gu = lat.pi_backward(w)
+    fdmu = (fwd(mu=MU + H) - fwd(mu=MU - H)) / (2 * H)
+    fdka = (fwd(kappa=KAPPA + H) - fwd(kappa=KAPPA - H)) / (2 * H)
+    D = seeded(99, 72 * vol)
+    fdu = (np.dot(fwd(gg=g + H * D), w) - np.dot(fwd(gg=g - H * D), w)) / (2 * H)
+    errs = {
+        "dPi/dmu": np.linalg.norm(dmu_t - fdmu) / np.linalg.norm(fdmu),
+        "dPi/dkappa": np.linalg.norm(dka_t - fdka) / np.linalg.norm(fdka),
+        "dL/dmu": abs(dmu - np.dot(fdmu, w)) / abs(dmu),
+        "dL/dkappa": abs(dka - np.dot(fdka, w)) / abs(dka),
+        "dL/dU.D": abs(np.dot(gu, D) - fdu) / abs(fdu),
+    }
+    print("\nC4 12^3x24 gradient relative errors: " +
+          ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
+    lat.close()
+    assert max(errs.values()) < 1e-6
