@@ -28,6 +28,7 @@ _D = ctypes.c_double
 _L = ctypes.c_long
 _IP = ctypes.POINTER(ctypes.c_int)
 _DP = ctypes.POINTER(ctypes.c_double)
+_U32P = ctypes.POINTER(ctypes.c_uint32)
 
 
 class SolverParams(ctypes.Structure):
@@ -90,6 +91,16 @@ SIGNATURES = {
     "cvcb_cvc_ward": (_I, [_P, _P, _P]),
     "cvcb_p2gg_seq_source": (_I, [_P, _P, _P, _I, _P, _I, _I]),
     "cvcb_plaquette": (_I, [_P, _P, _P]),
+    "cvcb_crc32": (_I, [ctypes.c_uint32, _P, ctypes.c_size_t, _U32P]),
+    "cvcb_dml_checksum_accum": (_I, [_U32P, ctypes.c_uint64, _P, ctypes.c_size_t]),
+    "cvcb_read_lime_gauge_field_doubleprec": (_I, [ctypes.c_char_p, _P, _I, _I, _I, _I, _U32P]),
+    "cvcb_write_lime_gauge_field": (_I, [ctypes.c_char_p, _P, _I, _I, _I, _I, _I, _U32P]),
+    "cvcb_read_lime_spinor": (_I, [_P, ctypes.c_char_p, _I, _I, _I, _I, _I, _U32P]),
+    "cvcb_write_lime_spinor": (_I, [_P, ctypes.c_char_p, _I, _I, _I, _I, _I, _I, _U32P]),
+    "cvcb_write_propagator": (_I, [_P, ctypes.c_char_p, _I, _I, _I, _I, _I, _U32P]),
+    "cvcb_write_lime_contraction": (_I, [_P, ctypes.c_char_p, _I, _I, ctypes.c_char_p, _I, _I,
+                                         _I, _I, _I, _I, _U32P]),
+    "cvcb_read_lime_contraction": (_I, [_P, ctypes.c_char_p, _I, _I, _I, _I, _I, _I, _U32P]),
     "cvcb_pi_forward": (_I, [_P, _I, ctypes.POINTER(SolverParams), _D, _P, _P]),
     "cvcb_pi_tangent": (_I, [_P, _I, _P]),
     "cvcb_pi_backward": (_I, [_P, _P, _P, _P, _P]),

@@ -24,6 +24,9 @@
 #ifndef CVCB_H
 #define CVCB_H
 
+#include <stddef.h>
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -324,6 +327,63 @@ int cvcb_pi_backward(cvcb_lattice *lat, const double *weights, double *dL_dU, do
 
 /* Plaquette <Re tr U_munu>/(18 V) and link sum (cvc_utils.c:384-436). */
 int cvcb_plaquette(cvcb_lattice *lat, double *plaq, double *linksum);
+
+/* ---------------------------------------------------------------------
+ * LIME / SciDAC / ILDG files (host memory, no GPU needed).  The reference
+ * reads and writes these through c-lime / lemon; the lattice extents it
+ * takes from globals are arguments here.  Fields are in CVC's layouts; every
+ * call returns the SciDAC checksum (suma, sumb) of the binary record in
+ * `checksum` (may be NULL).  Files are big-endian, 64- or 32-bit; readers
+ * take the precision from the record length.
+ * ------------------------------------------------------------------- */
+
+/* CRC-32 (zlib polynomial) of len bytes continuing from crc, as DML_crc32
+ * (DML_crc32.c). */
+int cvcb_crc32(uint32_t crc, const void *buf, size_t len, uint32_t *out);
+
+/* SciDAC checksum step (dml.c:22-50, DML_checksum_accum): sums[0] ^=
+ * rotl(crc, rank % 29), sums[1] ^= rotl(crc, rank % 31), crc = CRC-32 of the
+ * site's size bytes. */
+int cvcb_dml_checksum_accum(uint32_t sums[2], uint64_t rank, const void *buf, size_t size);
+
+/* Gauge field from the ildg-binary-data record of an ILDG file
+ * (io.c:202-343 read_lime_gauge_field_doubleprec; 32-bit files as
+ * read_lime_gauge_field_singleprec): gauge = 72*V doubles. */
+int cvcb_read_lime_gauge_field_doubleprec(const char *filename, double *gauge, int T, int LX,
+                                          int LY, int LZ, uint32_t checksum[2]);
+
+/* ILDG gauge file: ildg-format, ildg-binary-data, scidac-checksum records
+ * (gauge_io.c:198-340 write_lime_gauge_field); prec 64 or 32. */
+int cvcb_write_lime_gauge_field(const char *filename, const double *gauge, int T, int LX, int LY,
+                                int LZ, int prec, uint32_t checksum[2]);
+
+/* Dirac field from the position-th scidac-binary-data record
+ * (propagator_io.c:771-840 read_lime_spinor); s = 24*V doubles. */
+int cvcb_read_lime_spinor(double *s, const char *filename, int position, int T, int LX, int LY,
+                          int LZ, uint32_t checksum[2]);
+
+/* Appends (append != 0) or writes a scidac-binary-data record and its
+ * scidac-checksum (propagator_io.c:578-647 write_lime_spinor). */
+int cvcb_write_lime_spinor(const double *s, const char *filename, int append, int prec, int T,
+                           int LX, int LY, int LZ, uint32_t checksum[2]);
+
+/* etmc-propagator-format record followed by write_lime_spinor
+ * (propagator_io.c:125-132 write_propagator). */
+int cvcb_write_propagator(const double *s, const char *filename, int prec, int T, int LX, int LY,
+                          int LZ, uint32_t checksum[2]);
+
+/* N-component contraction (N complex numbers per site, CVC site order; Pi
+ * is N = 16): cvc_contraction-format, scidac-binary-data and scidac-checksum
+ * records (contractions_io.c:56-137,338-420 write_lime_contraction, the
+ * lemon variant; the reference's plain-LIME variant is a stub). */
+int cvcb_write_lime_contraction(const double *s, const char *filename, int prec, int N,
+                                const char *type, int gid, int sid, int T, int LX, int LY, int LZ,
+                                uint32_t checksum[2]);
+
+/* The position-th scidac-binary-data record as an N-component contraction
+ * (contractions_io.c:140-235,420-480 read_lime_contraction). */
+int cvcb_read_lime_contraction(double *s, const char *filename, int N, int position, int T, int LX,
+                               int LY, int LZ, uint32_t checksum[2]);
 
 #ifdef __cplusplus
 }

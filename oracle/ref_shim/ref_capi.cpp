@@ -22,6 +22,7 @@
 #include "Q_phi.h"
 #include "invert_Qtm.h"
 #include "ranlxd.h"
+#include "dml.h"
 
 using namespace cvc;
 
@@ -135,4 +136,18 @@ void ref_get_filename(char *fn, int nu, int sc, int sign, const char *prefix, co
 
 extern "C" void ref_get_work(int i, double *out) {
   memcpy(out, g_spinor_field[i], (size_t)24 * VOLUME * sizeof(double));
+}
+
+/* SciDAC checksum step of the reference (dml.c) and its CRC-32 (DML_crc32.c). */
+extern "C" void ref_dml_checksum_accum(unsigned int *sums, unsigned int rank, const void *buf,
+                                       size_t size) {
+  DML_Checksum c;
+  c.suma = sums[0];
+  c.sumb = sums[1];
+  DML_checksum_accum(&c, (DML_SiteRank)rank, (char *)buf, size);
+  sums[0] = c.suma;
+  sums[1] = c.sumb;
+}
+extern "C" unsigned int ref_dml_crc32(unsigned int crc, const void *buf, size_t len) {
+  return DML_crc32(crc, (const unsigned char *)buf, len);
 }
