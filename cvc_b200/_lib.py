@@ -91,6 +91,14 @@ SIGNATURES = {
     "cvcb_cvc_ward": (_I, [_P, _P, _P]),
     "cvcb_p2gg_seq_source": (_I, [_P, _P, _P, _I, _P, _I, _I]),
     "cvcb_plaquette": (_I, [_P, _P, _P]),
+    "cvcb_pi_momentum": (_I, [_P, _P, _I, _P, _P]),
+    "cvcb_BHn": (_I, [_P, _P, _P, _I]),
+    "cvcb_BH": (_I, [_P, _P, _P]),
+    "cvcb_BH2": (_I, [_P, _P, _P]),
+    "cvcb_BH3": (_I, [_P, _P, _P]),
+    "cvcb_BH5": (_I, [_P, _P, _P]),
+    "cvcb_BH7": (_I, [_P, _P, _P]),
+    "cvcb_gamma5_BdagH4_gamma5": (_I, [_P, _P, _P, _P]),
     "cvcb_crc32": (_I, [ctypes.c_uint32, _P, ctypes.c_size_t, _U32P]),
     "cvcb_dml_checksum_accum": (_I, [_U32P, ctypes.c_uint64, _P, ctypes.c_size_t]),
     "cvcb_read_lime_gauge_field_doubleprec": (_I, [ctypes.c_char_p, _P, _I, _I, _I, _I, _U32P]),

@@ -255,6 +255,40 @@ class Lattice:
                                                           ptr(dka)))
         return float(dmu[0]), float(dka[0]), gu
 
+    def pi_momentum(self, conn, source_site, contact=None, out=None):
+        """Pi_mu_nu(q) with midpoint phases and the contact term subtracted
+        (32*V doubles, momenta in lexicographic order)."""
+        if out is None:
+            out = np.zeros(32 * self.VOLUME)
+        ct = None if contact is None else np.ascontiguousarray(contact, np.float64)
+        _check("pi_momentum", self._lib.cvcb_pi_momentum(self._h, ptr(conn), int(source_site),
+                                                          ptr(ct), ptr(out)))
+        return out
+
+    # -- hopping-parameter expansion (Q_phi.c:536-781) -------------------
+    def BHn(self, xi, phi, n):
+        """xi = (B H)^n phi; phi is overwritten as the reference does."""
+        _check("BHn", self._lib.cvcb_BHn(self._h, ptr(xi), ptr(phi), int(n)))
+
+    def BH(self, xi, phi):
+        _check("BH", self._lib.cvcb_BH(self._h, ptr(xi), ptr(phi)))
+
+    def BH2(self, xi, phi):
+        _check("BH2", self._lib.cvcb_BH2(self._h, ptr(xi), ptr(phi)))
+
+    def BH3(self, xi, phi):
+        _check("BH3", self._lib.cvcb_BH3(self._h, ptr(xi), ptr(phi)))
+
+    def BH5(self, xi, phi):
+        _check("BH5", self._lib.cvcb_BH5(self._h, ptr(xi), ptr(phi)))
+
+    def BH7(self, xi, phi):
+        _check("BH7", self._lib.cvcb_BH7(self._h, ptr(xi), ptr(phi)))
+
+    def gamma5_BdagH4_gamma5(self, xi, phi, work):
+        _check("gamma5_BdagH4_gamma5",
+               self._lib.cvcb_gamma5_BdagH4_gamma5(self._h, ptr(xi), ptr(phi), ptr(work)))
+
     def plaquette(self):
         pl = np.zeros(1)
         ls = np.zeros(2)

@@ -325,6 +325,35 @@ int cvcb_pi_tangent(cvcb_lattice *lat, int parameter, double *dconn);
 int cvcb_pi_backward(cvcb_lattice *lat, const double *weights, double *dL_dU, double *dL_dmu,
                      double *dL_dkappa);
 
+/* Momentum-space Pi_mu_nu(q) (the step after the path in the reference's
+ * momentum-space programs), with the conserved currents at their link
+ * midpoints and the contact term subtracted:
+ *   pimom_mu_nu(q) = e^{i q.y} e^{-i q_mu/2} e^{i q_nu/2} sum_x e^{-i q.x}
+ *                    conn_mu_nu(x) - delta_mu_nu contact_nu,
+ * q_mu = 2 pi k_mu / L_mu, output at pimom[2*(16*k + 4*mu + nu) + re/im] with
+ * k = ((k_t*LX + k_x)*LY + k_y)*LZ + k_z; y = source_site (lexicographic);
+ * contact (8 doubles, as from cvcb_cvc_contract) may be NULL (no
+ * subtraction).  Then sum_mu 2 sin(q_mu/2) pimom_mu_nu(q) = 0, the Ward
+ * identity of cvc_exact2_xspace.c:928-1008. */
+int cvcb_pi_momentum(cvcb_lattice *lat, const double *conn, int source_site,
+                     const double *contact, double *pimom);
+
+/* Hopping-parameter expansion (Q_phi.c:536-781), B = (1 - i 2 kappa mu g5) /
+ * (1 + (2 kappa mu)^2) as in mul_one_pm_imu_inv(+1), H = the hop sum of
+ * Hopping.  The reference's side effects on phi are kept:
+ *   cvcb_BHn: xi = (B H)^n phi; for n >= 2 phi becomes (B H)^(2 [n/2]) phi
+ *   (Q_phi.c:753-781).  cvcb_BH, _BH3, _BH5, _BH7: n = 1, 3, 5, 7
+ *   (Q_phi.c:598-751).  cvcb_BH2: phi = (B H)^2 phi, xi = B H phi
+ *   (Q_phi.c:683-702).  cvcb_gamma5_BdagH4_gamma5: xi = g5 (B^+ H)^4 g5 phi,
+ *   work = (B^+ H)^3 g5 phi, phi unchanged (Q_phi.c:536-570). */
+int cvcb_BHn(cvcb_lattice *lat, double *xi, double *phi, int n);
+int cvcb_BH(cvcb_lattice *lat, double *xi, double *phi);
+int cvcb_BH2(cvcb_lattice *lat, double *xi, double *phi);
+int cvcb_BH3(cvcb_lattice *lat, double *xi, double *phi);
+int cvcb_BH5(cvcb_lattice *lat, double *xi, double *phi);
+int cvcb_BH7(cvcb_lattice *lat, double *xi, double *phi);
+int cvcb_gamma5_BdagH4_gamma5(cvcb_lattice *lat, double *xi, const double *phi, double *work);
+
 /* Plaquette <Re tr U_munu>/(18 V) and link sum (cvc_utils.c:384-436). */
 int cvcb_plaquette(cvcb_lattice *lat, double *plaq, double *linksum);
 

@@ -151,3 +151,14 @@ extern "C" void ref_dml_checksum_accum(unsigned int *sums, unsigned int rank, co
 extern "C" unsigned int ref_dml_crc32(unsigned int crc, const void *buf, size_t len) {
   return DML_crc32(crc, (const unsigned char *)buf, len);
 }
+
+/* Hopping-parameter-expansion helpers of the reference (Q_phi.c:536-781). */
+extern "C" void ref_BHn(double *xi, double *phi, int n) { BHn(xi, phi, n); }
+extern "C" void ref_BH(double *xi, double *phi) { BH(xi, phi); }
+extern "C" void ref_BH2(double *xi, double *phi) { BH2(xi, phi); }
+extern "C" void ref_BH3(double *xi, double *phi) { BH3(xi, phi); }
+extern "C" void ref_BH5(double *xi, double *phi) { BH5(xi, phi); }
+extern "C" void ref_BH7(double *xi, double *phi) { BH7(xi, phi); }
+extern "C" void ref_gamma5_BdagH4_gamma5(double *xi, double *phi, double *work) {
+  gamma5_BdagH4_gamma5(xi, phi, work);
+}

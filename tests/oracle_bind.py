@@ -271,6 +271,21 @@ class Reference:
         rc = fn(_p(x), _p(np.array(phi, dtype=np.float64, copy=True)), _D(prec), nmax, 1)
         return rc, x
 
+    def hpe(self, name, phi, *extra):
+        """Runs the reference's BHn / BH / BH2 / BH3 / BH5 / BH7 (extra = (n,)
+        for BHn) on copies; returns (xi, phi) after the call."""
+        xi = np.zeros(24 * self.V)
+        ph = np.array(phi, dtype=np.float64, copy=True)
+        getattr(self.lib, "ref_" + name)(_p(xi), _p(ph), *extra)
+        return xi, ph
+
+    def gamma5_BdagH4_gamma5(self, phi):
+        xi = np.zeros(24 * self.V)
+        work = np.zeros(24 * self.V)
+        ph = np.array(phi, dtype=np.float64, copy=True)
+        self.lib.ref_gamma5_BdagH4_gamma5(_p(xi), _p(ph), _p(work))
+        return xi, ph, work
+
     def plaquette(self):
         pl = np.zeros(1)
         self._quiet(lambda: self.lib.ref_plaquette(_p(pl)))

@@ -111,3 +111,17 @@ def test_stencil_timing_algorithmic_bytes():
     assert algorithmic_bytes(1, 1, 12, 12, dims) == 891_813_888
     assert algorithmic_bytes(2, 1, 12, 12, dims) == 2 * 891_813_888 + 2 * 1_274_019_840
     assert algorithmic_bytes(0, 0, 18, 1, dims) == 663_552 * (2 * 192 + 8 * 144)
+
+
+def test_tmlqcd_library_exports_the_wrapper_abi(cb):
+    """libcvcb200_tmlqcd.so exports every function of the tmLQCD wrapper
+    header (include/cvcb_tmlqcd.h, tmLQCD.h:46-54 of the reference)."""
+    from cvc_b200 import _lib
+    path = os.path.join(os.path.dirname(_lib.LIB_PATH), "libcvcb200_tmlqcd.so")
+    lib = ctypes.CDLL(path)
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(_lib.LIB_PATH)), "include",
+                            "cvcb_tmlqcd.h")).read()
+    names = set(re.findall(r"\bint\s+(tmLQCD_\w+)\s*\(", hdr))
+    assert len(names) == 7
+    for n in names:
+        assert hasattr(lib, n), n
