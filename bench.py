@@ -350,7 +350,10 @@ def main():
             for sc in range(12):
                 pin_b[12 * k + sc][24 * s + 2 * sc] = 1.0
         pin_x = [torch.zeros(24 * V, dtype=torch.float64).pin_memory() for _ in range(nrhs)]
-        ke = 1
+        # one untimed call sets up the pipeline's staging buffers and stream
+        st = lat.solve(pin_x, pin_b, params)
+        assert st.converged == nrhs
+        ke = max(1, args.steps)
         if world > 1:
             dist.barrier()
         t = time.perf_counter()
@@ -365,8 +368,10 @@ def main():
         result["e2e"] = {"value": world * nrhs / dt, "unit": "solves/s",
                          "h2d_bytes_per_step": nrhs * 24 * V * 8,
                          "d2h_bytes_per_step": nrhs * 24 * V * 8,
-                         "note": "host pinned buffers through cvcb_solve; copies and the "
-                                 "CVC<->device layout transforms inside the timed region"}
+                         "steps": ke,
+                         "note": "host pinned buffers through cvcb_solve (copies overlap the "
+                                 "solve on a second stream); copies and the CVC<->device layout "
+                                 "transforms inside the timed region"}
         del pin_b, pin_x
 
     # CPU baseline: the reference's own solver, serial, bounded sample

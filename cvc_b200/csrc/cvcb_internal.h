@@ -179,6 +179,10 @@ struct cvcb_lattice {
   double bc[4] = {1, 0, 0, 0};
   double phase[8] = {0};
   cudaStream_t stream = nullptr;
+  // second stream and events of the host<->device pipeline of cvcb_solve
+  // (created on first use)
+  cudaStream_t copy_stream = nullptr, copy_stream_out = nullptr;
+  cudaEvent_t pipe_ev[6] = {};
   bool have_gauge = false;
   double unitarity = -1.0;
   std::vector<double> gauge_host;  // raw CVC-layout copy (for re-phasing)
@@ -234,6 +238,11 @@ enum BufSlot {
   SLOT_CONN,
   SLOT_PROPS,
   SLOT_MIX0,
+  // double-buffered raw-layout staging of the solve pipeline (host fields)
+  SLOT_PIPE_IN0 = 56,
+  SLOT_PIPE_IN1,
+  SLOT_PIPE_OUT0,
+  SLOT_PIPE_OUT1,
   SLOT_NUM = 64
 };
 

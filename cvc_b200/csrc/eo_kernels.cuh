@@ -16,6 +16,8 @@
 
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 #include "cvcb_internal.h"
 #include "spinor_ops.cuh"
 
@@ -51,6 +53,11 @@ struct F32Acc {
     }
     return s;
   }
+  // unscaled load (FP32 storage has no per-site scale: nm = 1)
+  __device__ __forceinline__ Spinor<float> load_raw(int r, int j, float &nm) const {
+    nm = 1.f;
+    return load(r, j);
+  }
   __device__ __forceinline__ void store(int r, int j, const Spinor<float> &s) const {
     float4 *q = p + r * rstride + j;
 #pragma unroll
@@ -68,8 +75,16 @@ struct F16Acc {
   float *norm;
   size_t stride, rstride;
   __device__ __forceinline__ Spinor<float> load(int r, int j) const {
+    float nm;
+    Spinor<float> s = load_raw(r, j, nm);
+#pragma unroll
+    for (int c = 0; c < 12; ++c) s.c[c / 3][c % 3] = nm * s.c[c / 3][c % 3];
+    return s;
+  }
+  // the stored halves as floats, and the site's scale (value = half * nm)
+  __device__ __forceinline__ Spinor<float> load_raw(int r, int j, float &nm) const {
     const uint4 *q = p + r * rstride + j;
-    const float nm = __ldg(norm + r * stride + j);
+    nm = __ldg(norm + r * stride + j);
     Spinor<float> s;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -79,7 +94,7 @@ struct F16Acc {
       for (int m = 0; m < 4; ++m) {
         const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w[m]));
         const int c = 4 * k + m;
-        s.c[c / 3][c % 3] = cx(f.x * nm, f.y * nm);
+        s.c[c / 3][c % 3] = cx(f.x, f.y);
       }
     }
     return s;
@@ -272,8 +287,20 @@ __device__ __forceinline__ Link<R> phased_link(const LF &lk, int mu, int j) {
   return W;
 }
 
+// Launch bounds: (256 threads, min resident blocks) caps registers at
+// 65536 / (256 * blocks).  Measured at 24^3x48, 12 rhs: the FP32-arithmetic
+// sweep with one rhs per thread runs best at 80 registers (3 blocks: 1.23 ms
+// per M^+M, with a few spills to L1); a bound of 1 block lets the compiler
+// take 176 registers and costs 46 %; 4 blocks (64 registers) spills too
+// much.  More rhs per thread need more registers.  FP64 sweeps keep the
+// plain thread bound (the compiler then uses about 150 registers).
+template <int NR>
+struct HopMinBlocks {
+  static constexpr int value = NR == 1 ? 3 : NR <= 3 ? 2 : 1;
+};
+
 template <class SF, class LF, int NR, bool G5IN, bool G5HOP, bool AUX>
-__global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop(HopArgs<SF, LF> A) {
+__device__ __forceinline__ void eo_hop_body(const HopArgs<SF, LF> &A) {
   using R = typename SF::R;
   const int r0 = (blockIdx.x * blockDim.y + threadIdx.y) * NR;
   const Geom &g = A.eg.g;
@@ -350,6 +377,17 @@ __global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop(HopArgs<SF, LF> A) {
   }
 }
 
+template <class SF, class LF, int NR, bool G5IN, bool G5HOP, bool AUX>
+__global__ void __launch_bounds__(kHopMaxThreads, HopMinBlocks<NR>::value)
+    k_eo_hop(HopArgs<SF, LF> A) {
+  eo_hop_body<SF, LF, NR, G5IN, G5HOP, AUX>(A);
+}
+
+template <class LF, bool G5IN, bool G5HOP, bool AUX>
+__global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop64(HopArgs<F64Acc, LF> A) {
+  eo_hop_body<F64Acc, LF, 1, G5IN, G5HOP, AUX>(A);
+}
+
 // ---- two right-hand sides per thread in packed FP32x2 arithmetic -----------
 // Lane x of every float2 belongs to rhs a, lane y to rhs b.  The link is the
 // same for both, so each complex multiply-add of the link product is two
@@ -380,6 +418,27 @@ __device__ __forceinline__ HalfPair pair_half(const HalfSpinor<float> &a, const 
       h.c[s][c].im = make_float2(a.c[s][c].im, b.c[s][c].im);
     }
   return h;
+}
+
+// Per-site scales of FP16+norm storage, applied after the projection to the
+// 12 values of the half-spinor pair (packed) instead of 2 x 24 components;
+// FP32 storage has none.
+template <class SF>
+__device__ __forceinline__ HalfPair scale_pair(const HalfPair &h, float na, float nb) {
+  if constexpr (std::is_same<SF, F32Acc>::value) {
+    return h;
+  } else {
+    const float2 n = make_float2(na, nb);
+    HalfPair o;
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        o.c[s][c].re = __fmul2_rn(n, h.c[s][c].re);
+        o.c[s][c].im = __fmul2_rn(n, h.c[s][c].im);
+      }
+    return o;
+  }
 }
 
 // u = W h (dag = false) or W^+ h (dag = true), both rhs at once
@@ -483,7 +542,7 @@ __device__ __forceinline__ void accum_recon_pair(int mu, int s, SpinorPair &acc,
 
 // Packed-pair stencil: thread = (site, rhs pair); same sweep as k_eo_hop.
 template <class SF, class LF, bool G5IN, bool G5HOP, bool AUX>
-__global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop_x2(HopArgs<SF, LF> A) {
+__global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_x2(HopArgs<SF, LF> A) {
   static_assert(sizeof(typename SF::R) == 4, "packed pairs need FP32 arithmetic");
   const int ra = (blockIdx.x * blockDim.y + threadIdx.y) * 2;
   if (ra >= A.nrhs) return;
@@ -509,23 +568,25 @@ __global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop_x2(HopArgs<SF, LF> A)
       {  // backward: (1 + g_mu) U_mu(x-mu)^+ in(x-mu)
         const int j = nb_lex(g, cd, mu, -1) >> 1;
         const Link<float> W = phased_link<float>(A.links, mu, qoff + j);
-        Spinor<float> fa = A.in.load(ra, j), fb = A.in.load(rb, j);
+        float na, nb;
+        Spinor<float> fa = A.in.load_raw(ra, j, na), fb = A.in.load_raw(rb, j, nb);
         if (G5IN) {
           g5_inplace(fa);
           g5_inplace(fb);
         }
-        const HalfPair h = pair_half(project(mu, +1, fa), project(mu, +1, fb));
+        const HalfPair h = scale_pair<SF>(pair_half(project(mu, +1, fa), project(mu, +1, fb)), na, nb);
         accum_recon_pair(mu, +1, acc, link_mul_pair<true>(W, h));
       }
       {  // forward: (1 - g_mu) U_mu(x) in(x+mu)
         const int j = nb_lex(g, cd, mu, +1) >> 1;
         const Link<float> W = phased_link<float>(A.links, mu, p * g.Vh + i);
-        Spinor<float> fa = A.in.load(ra, j), fb = A.in.load(rb, j);
+        float na, nb;
+        Spinor<float> fa = A.in.load_raw(ra, j, na), fb = A.in.load_raw(rb, j, nb);
         if (G5IN) {
           g5_inplace(fa);
           g5_inplace(fb);
         }
-        const HalfPair h = pair_half(project(mu, -1, fa), project(mu, -1, fb));
+        const HalfPair h = scale_pair<SF>(pair_half(project(mu, -1, fa), project(mu, -1, fb)), na, nb);
         accum_recon_pair(mu, -1, acc, link_mul_pair<false>(W, h));
       }
     }
@@ -569,7 +630,7 @@ __host__ __device__ constexpr size_t staged_smem_bytes(int bx) {
 }
 
 template <class SF, class LF, bool G5IN, bool G5HOP, bool AUX>
-__global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop_staged(HopArgs<SF, LF> A) {
+__device__ __forceinline__ void eo_hop_staged_body(const HopArgs<SF, LF> &A) {
   using R = typename SF::R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int bx = blockDim.x, tx = threadIdx.x, ty = threadIdx.y;
@@ -638,6 +699,17 @@ __global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop_staged(HopArgs<SF, LF
     }
     __syncthreads();  // the next site block overwrites the staged links
   }
+}
+
+// FP32 arithmetic: capped at 128 registers (2 blocks of 256); FP64: the
+// plain thread bound.
+template <class SF, class LF, bool G5IN, bool G5HOP, bool AUX>
+__global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_staged(HopArgs<SF, LF> A) {
+  eo_hop_staged_body<SF, LF, G5IN, G5HOP, AUX>(A);
+}
+template <class LF, bool G5IN, bool G5HOP, bool AUX>
+__global__ void __launch_bounds__(kHopMaxThreads) k_eo_hop_staged64(HopArgs<F64Acc, LF> A) {
+  eo_hop_staged_body<F64Acc, LF, G5IN, G5HOP, AUX>(A);
 }
 
 }  // namespace cvcb

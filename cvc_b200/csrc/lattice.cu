@@ -281,6 +281,13 @@ int cvcb_lattice_destroy(cvcb_lattice *L) {
   cudaFree(L->red_counter);
   cudaFree(L->red_result);
   cudaFree(L->scal);
+  for (cudaStream_t cs : {L->copy_stream, L->copy_stream_out})
+    if (cs) {
+      cudaStreamSynchronize(cs);
+      cudaStreamDestroy(cs);
+    }
+  for (cudaEvent_t e : L->pipe_ev)
+    if (e) cudaEventDestroy(e);
   if (L->stream) cudaStreamDestroy(L->stream);
   delete L;
   return CVCB_OK;

@@ -131,29 +131,25 @@ struct EpiAlphaB {
   }
 };
 
-// x_s += alpha p; r_s -= alpha Ap; rr_new = |r_s|^2; beta = rr_new / rr
-template <class SF, class XF>
+// r_s -= alpha Ap; rr_new = |r_s|^2; beta = rr_new / rr.  The x update
+// waits for k_p_upd, which reads p anyway: 3 instead of 6 field passes here
+// for 2 more there.
+template <class SF>
 struct RedUpdate {
-  SF p, Ap, rs;
-  XF xs;
+  SF Ap, rs;
   Scal S;
   __device__ double operator()(int r, int s) const {
     using R = typename SF::R;
-    using RX = typename XF::R;
-    const double a = S.alpha[r];
-    const Spinor<R> pv = p.load(r, s), apv = Ap.load(r, s);
+    const R a = (R)S.alpha[r];
+    const Spinor<R> apv = Ap.load(r, s);
     Spinor<R> rv = rs.load(r, s);
-    Spinor<RX> xv = xs.load(r, s);
 #pragma unroll
     for (int k = 0; k < 4; ++k)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        xv.c[k][c].re += (RX)(a * pv.c[k][c].re);
-        xv.c[k][c].im += (RX)(a * pv.c[k][c].im);
-        rv.c[k][c].re -= (R)(a * apv.c[k][c].re);
-        rv.c[k][c].im -= (R)(a * apv.c[k][c].im);
+        rv.c[k][c].re -= a * apv.c[k][c].re;
+        rv.c[k][c].im -= a * apv.c[k][c].im;
       }
-    xs.store(r, s, xv);
     rs.store(r, s, rv);
     return norm2(rv);
   }
@@ -166,20 +162,28 @@ struct EpiBetaB {
   }
 };
 
-// p = r_s + beta p
-template <class SF>
-__global__ void k_p_upd(SF p, SF rs, Scal S, int nsites, int nrhs) {
+// x_s += alpha p; p = r_s + beta p
+template <class SF, class XF>
+__global__ void k_p_upd(SF p, SF rs, XF xs, Scal S, int nsites, int nrhs) {
   using R = typename SF::R;
+  using RX = typename XF::R;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int r = blockIdx.y;
   if (s >= nsites || r >= nrhs || S.done[r]) return;
   const R b = (R)S.beta[r];
+  const RX a = (RX)S.alpha[r];
   const Spinor<R> rv = rs.load(r, s);
   Spinor<R> pv = p.load(r, s);
+  Spinor<RX> xv = xs.load(r, s);
 #pragma unroll
   for (int k = 0; k < 4; ++k)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) pv.c[k][c] = rv.c[k][c] + b * pv.c[k][c];
+    for (int c = 0; c < 3; ++c) {
+      xv.c[k][c].re += a * (RX)pv.c[k][c].re;
+      xv.c[k][c].im += a * (RX)pv.c[k][c].im;
+      pv.c[k][c] = rv.c[k][c] + b * pv.c[k][c];
+    }
+  xs.store(r, s, xv);
   p.store(r, s, pv);
 }
 
@@ -467,7 +471,12 @@ struct Batch {
     if (packed) {
     } else if (by > 1 && sh.nr == 1) {
       // rows of the block share links staged in shared memory
-      auto kern = k_eo_hop_staged<AF, LL, G5IN, G5HOP, AUX>;
+      auto kern = [] {
+        if constexpr (sizeof(typename AF::R) == 8)
+          return k_eo_hop_staged64<LL, G5IN, G5HOP, AUX>;
+        else
+          return k_eo_hop_staged<AF, LL, G5IN, G5HOP, AUX>;
+      }();
       const size_t smem = staged_smem_bytes<typename AF::R>(sh.bx);
       static std::atomic<unsigned long long> attr_set{0};  // per instantiation, bit per device
       const unsigned long long bit = 1ull << (L->device & 63);
@@ -482,7 +491,7 @@ struct Batch {
       }
       kern<<<grid, block, smem, L->stream>>>(a);
     } else if constexpr (sizeof(typename AF::R) == 8) {
-      k_eo_hop<AF, LL, 1, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
+      k_eo_hop64<LL, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
     } else {
       switch (sh.nr) {
         case 2: k_eo_hop<AF, LL, 2, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
@@ -531,11 +540,11 @@ struct Batch {
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedPAp<SF>{p, Ap}, EpiAlphaB{S}, g.Vh, br,
                                                     S.done);
     CVCB_LAUNCHED(L);
-    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedUpdate<SF, XF>{p, Ap, rs, xs, S},
+    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedUpdate<SF>{Ap, rs, S},
                                                     EpiBetaB{S}, g.Vh, br, S.done);
     CVCB_LAUNCHED(L);
     dim3 eg((g.Vh + 127) / 128, n);
-    k_p_upd<<<eg, 128, 0, L->stream>>>(p, rs, S, g.Vh, n);
+    k_p_upd<<<eg, 128, 0, L->stream>>>(p, rs, xs, S, g.Vh, n);
     CVCB_LAUNCHED(L);
     return CVCB_OK;
   }
@@ -831,7 +840,8 @@ int tune_shape64(cvcb_lattice *L, Batch<SF, XF, LF> &B) {
 
 template <class SF, class XF, class LF>
 int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
-              const cvcb_solver_params *P, cvcb_solver_stats *st, LaunchShape *shape_out) {
+              const cvcb_solver_params *P, cvcb_solver_stats *st, LaunchShape *shape_out,
+              cudaEvent_t inputs_read = nullptr) {
   Batch<SF, XF, LF> B;
   CVCB_TRY(setup_batch(L, B, n));
   const Geom &g = L->g;
@@ -841,6 +851,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   dim3 rg(red_blocks_sites(g.Vh), n), rgf(red_blocks_sites(g.V), n);
 
   for (int i = 0; i < n; ++i) CVCB_TRY(spinor_in(L, B.b64 + i * fs, b[i], g.V));
+  if (inputs_read) CVCB_CUDA(cudaEventRecord(inputs_read, L->stream));
   CVCB_TRY(tune_shape(L, B, P->precision, P->link_recon, P->block_threads));
   if (sizeof(typename SF::R) != 8) CVCB_TRY(tune_shape64(L, B));
   if (shape_out) *shape_out = B.shape;
@@ -1183,6 +1194,72 @@ int tune_batch(cvcb_lattice *L, const cvcb_solver_params *P, int recon, int nrhs
   return CVCB_OK;
 }
 
+// Host-resident fields over several batches: one copy stream brings the
+// sources of batch k+1 into device staging (raw CVC layout) and another takes
+// the solutions of batch k-1 back to the host while batch k is solved, so the
+// PCIe traffic of both directions overlaps the solve.  Staging is double-buffered; events hand
+// each buffer between the streams (inputs consumed -> next prefetch,
+// outputs copied -> next write).
+template <class Run>
+int solve_pipelined(cvcb_lattice *L, double *const *x, const double *const *b, int nrhs, int nb,
+                    Run &run) {
+  const size_t fbytes = (size_t)L->g.V * 24 * sizeof(double);
+  if (!L->copy_stream) {
+    CVCB_CUDA(cudaStreamCreateWithFlags(&L->copy_stream, cudaStreamNonBlocking));
+    CVCB_CUDA(cudaStreamCreateWithFlags(&L->copy_stream_out, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : L->pipe_ev) CVCB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  cudaStream_t cs = L->copy_stream, co = L->copy_stream_out;
+  // events per buffer k%2: [0,1] inputs landed, [2,3] inputs read, [4,5] outputs copied out
+  cudaEvent_t *landed = L->pipe_ev, *read = L->pipe_ev + 2, *drained = L->pipe_ev + 4;
+  double *in[2], *out[2];
+  for (int k = 0; k < 2; ++k) {
+    void *a, *c;
+    CVCB_TRY(ensure_buffer(L, SLOT_PIPE_IN0 + k, fbytes * nb, &a));
+    CVCB_TRY(ensure_buffer(L, SLOT_PIPE_OUT0 + k, fbytes * nb, &c));
+    in[k] = static_cast<double *>(a);
+    out[k] = static_cast<double *>(c);
+  }
+  const int nbatch = (nrhs + nb - 1) / nb;
+  auto prefetch = [&](int k) -> int {
+    const int off = k * nb, n = std::min(nb, nrhs - off), s = k % 2;
+    if (k >= 2) CVCB_CUDA(cudaStreamWaitEvent(cs, read[s], 0));
+    for (int i = 0; i < n; ++i)
+      CVCB_CUDA(cudaMemcpyAsync(in[s] + (size_t)i * fbytes / sizeof(double), b[off + i], fbytes,
+                                cudaMemcpyHostToDevice, cs));
+    CVCB_CUDA(cudaEventRecord(landed[s], cs));
+    return CVCB_OK;
+  };
+  int rc = prefetch(0);
+  std::vector<double *> xs(nb);
+  std::vector<const double *> bs(nb);
+  for (int k = 0; k < nbatch && rc >= 0; ++k) {
+    const int off = k * nb, n = std::min(nb, nrhs - off), s = k % 2;
+    if (k + 1 < nbatch && (rc = prefetch(k + 1)) < 0) break;
+    for (int i = 0; i < n; ++i) {
+      bs[i] = in[s] + (size_t)i * fbytes / sizeof(double);
+      xs[i] = out[s] + (size_t)i * fbytes / sizeof(double);
+    }
+    CVCB_CUDA(cudaStreamWaitEvent(L->stream, landed[s], 0));
+    if (k >= 2) CVCB_CUDA(cudaStreamWaitEvent(L->stream, drained[s], 0));
+    rc = run(xs.data(), bs.data(), n, read[s]);
+    if (rc < 0) break;
+    // run() returned after its stream finished: the solutions are in out[s]
+    for (int i = 0; i < n; ++i)
+      CVCB_CUDA(cudaMemcpyAsync(x[off + i], xs[i], fbytes, cudaMemcpyDeviceToHost, co));
+    CVCB_CUDA(cudaEventRecord(drained[s], co));
+  }
+  cudaError_t e = cudaStreamSynchronize(cs);
+  const cudaError_t e2 = cudaStreamSynchronize(co);
+  if (e == cudaSuccess) e = e2;
+  if (rc < 0) return rc;
+  if (e != cudaSuccess) {
+    set_error("solve pipeline: %s", cudaGetErrorString(e));
+    return CVCB_ERR_CUDA;
+  }
+  return CVCB_OK;
+}
+
 int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int nrhs,
                   const cvcb_solver_params *P, cvcb_solver_stats *st) {
   if (!L->have_gauge) {
@@ -1221,18 +1298,25 @@ int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int
     }
   }
   st->batch_rhs = nb;
-  for (int off = 0; off < nrhs; off += nb) {
-    const int n = std::min(nb, nrhs - off);
-    int rc;
+  auto run = [&](double *const *xs, const double *const *bs, int n, cudaEvent_t read) {
     if (P->precision == CVCB_PREC_DOUBLE)
-      rc = run_batch<F64Acc, F64Acc, L64>(L, x + off, b + off, n, P, st, nullptr);
-    else if (P->precision == CVCB_PREC_SINGLE)
-      rc = recon == 12 ? run_batch<F32Acc, F32Acc, L32c>(L, x + off, b + off, n, P, st, nullptr)
-                       : run_batch<F32Acc, F32Acc, L32f>(L, x + off, b + off, n, P, st, nullptr);
-    else
-      rc = recon == 12 ? run_batch<F16Acc, F32Acc, L16c>(L, x + off, b + off, n, P, st, nullptr)
-                       : run_batch<F16Acc, F32Acc, L32f>(L, x + off, b + off, n, P, st, nullptr);
+      return run_batch<F64Acc, F64Acc, L64>(L, xs, bs, n, P, st, nullptr, read);
+    if (P->precision == CVCB_PREC_SINGLE)
+      return recon == 12 ? run_batch<F32Acc, F32Acc, L32c>(L, xs, bs, n, P, st, nullptr, read)
+                         : run_batch<F32Acc, F32Acc, L32f>(L, xs, bs, n, P, st, nullptr, read);
+    return recon == 12 ? run_batch<F16Acc, F32Acc, L16c>(L, xs, bs, n, P, st, nullptr, read)
+                       : run_batch<F16Acc, F32Acc, L32f>(L, xs, bs, n, P, st, nullptr, read);
+  };
+  bool host = nrhs > nb;
+  for (int i = 0; i < nrhs && host; ++i) host = !is_device_ptr(x[i]) && !is_device_ptr(b[i]);
+  if (host) {
+    const int rc = solve_pipelined(L, x, b, nrhs, nb, run);
     if (rc < 0) return rc;
+  } else {
+    for (int off = 0; off < nrhs; off += nb) {
+      const int rc = run(x + off, b + off, std::min(nb, nrhs - off), nullptr);
+      if (rc < 0) return rc;
+    }
   }
   return st->converged == nrhs ? CVCB_OK : CVCB_NO_CONVERGENCE;
 }

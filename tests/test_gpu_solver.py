@@ -163,3 +163,27 @@ def test_batched_solver_tiny_magnitudes(cb, prec):
         assert np.all(np.isfinite(b))
         assert rel_err(1e33 * b, a) < 1e-8
     lat.close()
+
+
+def test_host_fields_pipeline_matches_device_fields(cb, env):
+    """Host-resident fields over several batches take the copy/compute
+    pipeline (sources of the next batch and solutions of the previous one
+    move on a second stream); the results equal those of device-resident
+    fields solved batch by batch."""
+    torch = pytest.importorskip("torch")
+    lat, _, _ = env
+    V = lat.VOLUME
+    n = 19  # 3 batches of 8: two full, one ragged
+    bs = [seeded(100 + i, 24 * V) for i in range(n)]
+    p = cb.solver_defaults()
+    p.block_rhs = 8
+    xh = [np.zeros(24 * V) for _ in range(n)]
+    st = lat.solve(xh, bs, p)
+    assert st.converged == n and st.max_true_res <= 1e-10
+    xd = [torch.zeros(24 * V, dtype=torch.float64, device="cuda") for _ in range(n)]
+    bd = [torch.from_numpy(b).cuda() for b in bs]
+    st2 = lat.solve(xd, bd, p)
+    torch.cuda.synchronize()
+    assert st2.converged == n
+    for a, d in zip(xh, xd):
+        assert rel_err(a, d.cpu().numpy()) < 1e-14
