@@ -183,6 +183,9 @@ struct cvcb_lattice {
   // (created on first use)
   cudaStream_t copy_stream = nullptr, copy_stream_out = nullptr;
   cudaEvent_t pipe_ev[6] = {};
+  // mapped pinned mailbox for the solver's per-rhs control values (host and
+  // device addresses of the same memory), created on first use
+  double *mbox_host = nullptr, *mbox_dev = nullptr;
   bool have_gauge = false;
   double unitarity = -1.0;
   std::vector<double> gauge_host;  // raw CVC-layout copy (for re-phasing)

@@ -288,6 +288,7 @@ int cvcb_lattice_destroy(cvcb_lattice *L) {
     }
   for (cudaEvent_t e : L->pipe_ev)
     if (e) cudaEventDestroy(e);
+  if (L->mbox_host) cudaFreeHost(L->mbox_host);
   if (L->stream) cudaStreamDestroy(L->stream);
   delete L;
   return CVCB_OK;

@@ -374,6 +374,54 @@ struct RedResid {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Control values between host and device.  The per-rhs scalars the host
+// reads every chunk and the flags it sets do not use cudaMemcpyAsync: a small
+// copy shares the DMA engines with the field transfers of the solve pipeline
+// and would wait behind them.  Values come back through a mapped pinned
+// mailbox that a one-warp kernel writes; flags go down as kernel arguments.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct FlagArgs {
+  int v[kMaxBatch];
+};
+__global__ void k_put_flags(int *__restrict__ dst, FlagArgs f, int n) {
+  if ((int)threadIdx.x < n) dst[threadIdx.x] = f.v[threadIdx.x];
+}
+__global__ void k_fetch(double *__restrict__ dst, const double *__restrict__ src, int n) {
+  if ((int)threadIdx.x < n) dst[threadIdx.x] = src[threadIdx.x];
+}
+
+constexpr int kMailSlots = 4;  // hb2, rr, rhat2, spare
+
+int put_flags(cvcb_lattice *L, int *dev, const std::vector<int> &h, int n) {
+  FlagArgs f{};
+  for (int i = 0; i < n; ++i) f.v[i] = h[i];
+  k_put_flags<<<1, 32, 0, L->stream>>>(dev, f, n);
+  CVCB_LAUNCHED(L);
+  return CVCB_OK;
+}
+
+// n doubles from the device into mailbox slot `slot`; the values are in
+// mailbox(L, slot) once L->stream has been synchronised.
+int fetch(cvcb_lattice *L, const double *dev, int n, int slot) {
+  if (!L->mbox_host) {
+    CVCB_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&L->mbox_host),
+                            sizeof(double) * kMaxBatch * kMailSlots, cudaHostAllocMapped));
+    CVCB_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&L->mbox_dev), L->mbox_host, 0));
+  }
+  k_fetch<<<1, 32, 0, L->stream>>>(L->mbox_dev + slot * kMaxBatch, dev, n);
+  CVCB_LAUNCHED(L);
+  return CVCB_OK;
+}
+void mailbox(cvcb_lattice *L, int slot, std::vector<double> &out, int n) {
+  const volatile double *m = L->mbox_host + slot * kMaxBatch;
+  for (int i = 0; i < n; ++i) out[i] = m[i];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
 // The solver object for one batch
 // ---------------------------------------------------------------------------
 struct LaunchShape {
@@ -862,8 +910,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
                                                    EpiStore{bnorm2}, g.V, B.br, nullptr);
   CVCB_LAUNCHED(L);
   std::vector<double> hb2(n);
-  CVCB_CUDA(cudaMemcpyAsync(hb2.data(), bnorm2, n * sizeof(double), cudaMemcpyDeviceToHost,
-                            L->stream));
+  CVCB_TRY(fetch(L, bnorm2, n, 0));
   // b_hat = b_o + 1/2 H_oe A_ee^-1 b_e
   double ia, ib;
   B.ainv(B.mu, ia, ib);
@@ -881,10 +928,12 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   CVCB_LAUNCHED(L);
   std::vector<double> rr(n), rr_max(n), rhat2(n), ratio2(n), target2(n);
   std::vector<int> done(n, 0), iters(n, 0), since(n, 0), skip(n, 0), rst(n, 1);
-  CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
-  CVCB_CUDA(cudaMemcpyAsync(rhat2.data(), B.S.rhat2, n * sizeof(double), cudaMemcpyDeviceToHost,
-                            L->stream));
+  CVCB_TRY(fetch(L, B.S.rr, n, 1));
+  CVCB_TRY(fetch(L, B.S.rhat2, n, 2));
   CVCB_CUDA(cudaStreamSynchronize(L->stream));
+  mailbox(L, 0, hb2, n);
+  mailbox(L, 1, rr, n);
+  mailbox(L, 2, rhat2, n);
   const double margin = 0.5;
   for (int i = 0; i < n; ++i) {
     target2[i] = std::pow(P->tol * margin, 2) * hb2[i];
@@ -893,8 +942,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     if (!(hb2[i] > 0)) done[i] = 1;  // zero right-hand side: x = 0
     else if (rhat2[i] <= target2[i]) done[i] = 1;
   }
-  CVCB_CUDA(cudaMemcpyAsync(B.S.done, done.data(), n * sizeof(int), cudaMemcpyHostToDevice,
-                            L->stream));
+  CVCB_TRY(put_flags(L, B.S.done, done, n));
 
   // One CG iteration is captured in a CUDA graph; between two host checks the
   // graph is launched k times, k <= kmax, with k cut to the number of
@@ -983,9 +1031,9 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
       if (rc != CVCB_OK) break;
     }
     total_iter += chunk;
-    CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost,
-                              L->stream));
+    CVCB_TRY(fetch(L, B.S.rr, n, 1));
     CVCB_CUDA(cudaStreamSynchronize(L->stream));
+    mailbox(L, 1, rr, n);
     if (L->prof) CVCB_TRY(harvest(active));
     bool any = false;
     for (int i = 0; i < n; ++i) {
@@ -1005,8 +1053,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
       }
     }
     if (!any) continue;
-    CVCB_CUDA(cudaMemcpyAsync(B.ru_skip, skip.data(), n * sizeof(int), cudaMemcpyHostToDevice,
-                              L->stream));
+    CVCB_TRY(put_flags(L, B.ru_skip, skip, n));
     // keep the search direction: q = p - r_s now, p = r_s' + q (q orthogonalised
     // against r_s') after the update
     k_dir_strip<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.ru_skip, g.Vh, n);
@@ -1027,18 +1074,17 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
       restart = restart || !rst[i];
     }
     if (restart) {
-      CVCB_CUDA(cudaMemcpyAsync(B.rst_skip, rst.data(), n * sizeof(int), cudaMemcpyHostToDevice,
-                                L->stream));
+      CVCB_TRY(put_flags(L, B.rst_skip, rst, n));
       k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.rst_skip, g.Vh, n);
       CVCB_LAUNCHED(L);
       for (int i = 0; i < n; ++i) nrestart += !rst[i];
     }
     ++nru;
-    CVCB_CUDA(cudaMemcpyAsync(rr.data(), B.S.rr, n * sizeof(double), cudaMemcpyDeviceToHost,
-                              L->stream));
-    CVCB_CUDA(cudaMemcpyAsync(rhat2.data(), B.S.rhat2, n * sizeof(double), cudaMemcpyDeviceToHost,
-                              L->stream));
+    CVCB_TRY(fetch(L, B.S.rr, n, 1));
+    CVCB_TRY(fetch(L, B.S.rhat2, n, 2));
     CVCB_CUDA(cudaStreamSynchronize(L->stream));
+    mailbox(L, 1, rr, n);
+    mailbox(L, 2, rhat2, n);
     for (int i = 0; i < n; ++i) {
       if (skip[i]) continue;
       since[i] = 0;
@@ -1047,8 +1093,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
       if (rhat2[i] > 0) ratio2[i] = rr[i] / rhat2[i];
       if (rhat2[i] <= target2[i]) done[i] = 1;
     }
-    CVCB_CUDA(cudaMemcpyAsync(B.S.done, done.data(), n * sizeof(int), cudaMemcpyHostToDevice,
-                              L->stream));
+    CVCB_TRY(put_flags(L, B.S.done, done, n));
   }
   if (gexec) cudaGraphExecDestroy(gexec);
   for (auto &r : B.recs) {
@@ -1072,10 +1117,10 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   k_reduce_rhs<<<rgf, kRedThreads, 0, L->stream>>>(
       RedResid{B.f64full(B.t64), B.f64full(B.b64)}, EpiStore{B.S.rhat2}, g.V, B.br, nullptr);
   CVCB_LAUNCHED(L);
-  CVCB_CUDA(cudaMemcpyAsync(rhat2.data(), B.S.rhat2, n * sizeof(double), cudaMemcpyDeviceToHost,
-                            L->stream));
+  CVCB_TRY(fetch(L, B.S.rhat2, n, 2));
   for (int i = 0; i < n; ++i) CVCB_TRY(spinor_out(L, x[i], B.x64 + i * fs, g.V));
   CVCB_CUDA(cudaStreamSynchronize(L->stream));
+  mailbox(L, 2, rhat2, n);
   for (int i = 0; i < n; ++i) {
     const double rel = hb2[i] > 0 ? std::sqrt(rhat2[i] / hb2[i]) : 0.0;
     worst = std::max(worst, rel);
