@@ -49,29 +49,51 @@ int ensure_buffer(cvcb_lattice *L, int slot, size_t bytes, void **out) {
 }
 
 // ---------------------------------------------------------------------------
-// layout transforms (one thread per lexicographic site, 12 complex numbers)
+// layout transforms, tiled through shared memory: a block takes kTile
+// consecutive lexicographic sites, whose CVC-layout data (12 complex numbers
+// each) is one contiguous chunk -- read or written with consecutive threads on
+// consecutive addresses -- and moves them to or from the 12 component arrays
+// of the even/odd layout, where consecutive threads touch consecutive sites of
+// one parity.
 // ---------------------------------------------------------------------------
-__global__ void k_spinor_aos_to_eo(double2 *__restrict__ dst, const double2 *__restrict__ src,
-                                   Geom g, int nsites) {
-  const int lex = blockIdx.x * blockDim.x + threadIdx.x;
-  if (lex >= g.V) return;
-  const int eo = lex_to_eo(g, lex);
-  if (lex < nsites) {
-#pragma unroll
-    for (int k = 0; k < 12; ++k) dst[(size_t)k * g.V + eo] = src[(size_t)lex * 12 + k];
-  } else {
-#pragma unroll
-    for (int k = 0; k < 12; ++k) dst[(size_t)k * g.V + eo] = make_double2(0.0, 0.0);
+constexpr int kTile = 64;
+constexpr int kTilePad = 13;  // row pitch of the tile (12 + 1 against bank conflicts)
+
+// all V sites of dst are written: sites lex >= nsites become zero
+__global__ void __launch_bounds__(128) k_spinor_aos_to_eo(double2 *__restrict__ dst,
+                                                         const double2 *__restrict__ src, Geom g,
+                                                         int nsites) {
+  __shared__ double2 t[kTile * kTilePad];
+  const int base = blockIdx.x * kTile;
+  const int nloc = min(kTile, g.V - base);
+  for (int q = threadIdx.x; q < nloc * 12; q += blockDim.x) {
+    const int s = q / 12, k = q - 12 * s;
+    t[s * kTilePad + k] = base + s < nsites ? src[(size_t)base * 12 + q] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nloc * 12; q += blockDim.x) {
+    const int k = q / nloc, s = q - k * nloc;
+    dst[(size_t)k * g.V + lex_to_eo(g, base + s)] = t[s * kTilePad + k];
   }
 }
 
-__global__ void k_spinor_eo_to_aos(double2 *__restrict__ dst, const double2 *__restrict__ src,
-                                   Geom g, int nsites) {
-  const int lex = blockIdx.x * blockDim.x + threadIdx.x;
-  if (lex >= nsites) return;
-  const int eo = lex_to_eo(g, lex);
-#pragma unroll
-  for (int k = 0; k < 12; ++k) dst[(size_t)lex * 12 + k] = src[(size_t)k * g.V + eo];
+// sites lex < nsites of dst are written
+__global__ void __launch_bounds__(128) k_spinor_eo_to_aos(double2 *__restrict__ dst,
+                                                         const double2 *__restrict__ src, Geom g,
+                                                         int nsites) {
+  __shared__ double2 t[kTile * kTilePad];
+  const int base = blockIdx.x * kTile;
+  const int nloc = min(kTile, nsites - base);
+  if (nloc <= 0) return;
+  for (int q = threadIdx.x; q < nloc * 12; q += blockDim.x) {
+    const int k = q / nloc, s = q - k * nloc;
+    t[s * kTilePad + k] = src[(size_t)k * g.V + lex_to_eo(g, base + s)];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nloc * 12; q += blockDim.x) {
+    const int s = q / 12, k = q - 12 * s;
+    dst[(size_t)base * 12 + q] = t[s * kTilePad + k];
+  }
 }
 
 int spinor_in(cvcb_lattice *L, double2 *dst, const double *src, int nsites) {
@@ -86,7 +108,7 @@ int spinor_in(cvcb_lattice *L, double2 *dst, const double *src, int nsites) {
                               cudaMemcpyHostToDevice, L->stream));
     dsrc = static_cast<const double2 *>(st);
   }
-  k_spinor_aos_to_eo<<<(g.V + 127) / 128, 128, 0, L->stream>>>(dst, dsrc, g, nsites);
+  k_spinor_aos_to_eo<<<(g.V + kTile - 1) / kTile, 128, 0, L->stream>>>(dst, dsrc, g, nsites);
   CVCB_LAUNCHED(L);
   return CVCB_OK;
 }
@@ -94,14 +116,14 @@ int spinor_in(cvcb_lattice *L, double2 *dst, const double *src, int nsites) {
 int spinor_out(cvcb_lattice *L, double *dst, const double2 *src, int nsites) {
   const Geom &g = L->g;
   if (is_device_ptr(dst)) {
-    k_spinor_eo_to_aos<<<(g.V + 127) / 128, 128, 0, L->stream>>>(
+    k_spinor_eo_to_aos<<<(g.V + kTile - 1) / kTile, 128, 0, L->stream>>>(
         reinterpret_cast<double2 *>(dst), src, g, nsites);
     CVCB_LAUNCHED(L);
     return CVCB_OK;
   }
   void *st;
   CVCB_TRY(ensure_buffer(L, SLOT_STAGE_B, (size_t)g.V * 24 * sizeof(double), &st));
-  k_spinor_eo_to_aos<<<(g.V + 127) / 128, 128, 0, L->stream>>>(static_cast<double2 *>(st), src,
+  k_spinor_eo_to_aos<<<(g.V + kTile - 1) / kTile, 128, 0, L->stream>>>(static_cast<double2 *>(st), src,
                                                                   g, nsites);
   CVCB_LAUNCHED(L);
   CVCB_CUDA(cudaMemcpyAsync(dst, st, (size_t)nsites * 24 * sizeof(double),
