@@ -317,7 +317,8 @@ def main():
             "max_true_residual": worst_res,
         },
         "roofline": {
-            "kernel": "k_eo_hop (batched even/odd stencil sweep, "
+            "kernel": ["k_eo_hop", "k_eo_hop_staged", "k_eo_hop_x2"][shape[3].value] +
+                      " (batched even/odd stencil sweep, "
                       f"{args.precision}, {params.link_recon}-real links)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "traffic": traffic,

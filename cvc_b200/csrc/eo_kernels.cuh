@@ -263,7 +263,24 @@ struct HopArgs {
   double d1a, d1b;  // D1 = d1a + i d1b g5
   double d2a, d2b;  // D2 = d2a + i d2b g5
   double c;         // hop coefficient
+  // optional (k_eo_hop_x2 only): per-warp partial sums of Re <dotp, out>,
+  // dot_part[rhs * dot_np + warp], warp = site block * (blockDim.x / 32) +
+  // warp in the row; null = off
+  SF dotp;
+  double *dot_part;
+  int dot_np;
 };
+
+// Re <a, b> of two sites, accumulated in FP64
+__device__ __forceinline__ double redot_site(const Spinor<float> &a, const Spinor<float> &b) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      s += (double)a.c[k][c].re * b.c[k][c].re + (double)a.c[k][c].im * b.c[k][c].im;
+  return s;
+}
 
 // Thread mapping: each thread handles one output site for NR right-hand
 // sides; blockDim.y groups of NR share the block.  The link of every
@@ -556,7 +573,8 @@ __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_x2(HopArgs<SF, LF>
   const int qoff = (1 - p) * g.Vh;
   for (int sb = blockIdx.y; sb * (int)blockDim.x < g.Vh; sb += gridDim.y) {
     const int i = sb * blockDim.x + threadIdx.x;
-    if (i >= g.Vh) return;
+    double da = 0.0, db = 0.0;  // Re <dotp, out> of this site, rhs a and b
+    if (i < g.Vh) {
     const SiteCoord cd = site_coord(g, p, i);
     SpinorPair acc;
 #pragma unroll
@@ -612,7 +630,21 @@ __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_x2(HopArgs<SF, LF>
 #pragma unroll
           for (int q = 0; q < 3; ++q) o.c[s][q] = o.c[s][q] + x.c[s][q];
       }
+      if (A.dot_part) (lane == 0 ? da : db) = redot_site(A.dotp.load(r, i), o);
       A.out.store(r, i, o);
+    }
+    }  // i < Vh
+    if (A.dot_part) {  // the whole warp is here: one row, warp-aligned block width
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        da += __shfl_down_sync(0xffffffffu, da, o);
+        db += __shfl_down_sync(0xffffffffu, db, o);
+      }
+      if ((threadIdx.x & 31) == 0) {
+        const int w = sb * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        A.dot_part[(size_t)ra * A.dot_np + w] = da;
+        if (has_b) A.dot_part[(size_t)rb * A.dot_np + w] = db;
+      }
     }
   }
 }

@@ -131,6 +131,20 @@ struct EpiAlphaB {
   }
 };
 
+// Sum of the per-warp partials of <p, Ap> that the last sweep of M^+M wrote
+// (fixed order: deterministic), then the epilogue (alpha).
+template <class E>
+__global__ void __launch_bounds__(kRedThreads)
+    k_dot_finish(const double *__restrict__ part, int np, E e, const int *__restrict__ skip) {
+  const int r = blockIdx.x;
+  if (skip && skip[r]) return;
+  __shared__ double sh[1][kRedThreads / 32];
+  double v[1] = {0.0};
+  for (int k = threadIdx.x; k < np; k += kRedThreads) v[0] += part[(size_t)r * np + k];
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) e(r, v[0]);
+}
+
 // r_s -= alpha Ap; rr_new = |r_s|^2; beta = rr_new / rr.  The x update
 // waits for k_p_upd, which reads p anyway: 3 instead of 6 field passes here
 // for 2 more there.
@@ -469,6 +483,8 @@ struct Batch {
   void *xs_mem;
   size_t xs_bytes;
   Scal S;
+  double *dot_part = nullptr;  // [rhs][dot_np] partials of <p, Ap> (fused into the stencil)
+  int dot_np = 0;
   int *ru_skip;   // per rhs: 1 = skip in the reliable update
   int *rst_skip;  // per rhs: 0 = restart the direction from the residual
   BatchRed br;
@@ -490,10 +506,22 @@ struct Batch {
   }
   F64Acc f64full(double2 *base) const { return F64Acc{base, (size_t)g.V, (size_t)12 * g.V}; }
 
+  // With dot_part (packed kernel only, warp-aligned blocks), the sweep also
+  // writes per-warp partials of Re <dotp, out> (dot_np per rhs).
   template <class AF, class LL, bool G5IN, bool G5HOP, bool AUX>
   int hop(AF out, AF in, AF aux, LL lk, int parity, const int *done, double d1a, double d1b,
-          double d2a, double d2b, double c) {
+          double d2a, double d2b, double c, double *dot_part = nullptr, const AF *dotp = nullptr) {
     HopArgs<AF, LL> a{out, in, aux, lk, EoGeom{g, parity}, n, done, d1a, d1b, d2a, d2b, c};
+    if (dot_part) {
+      if (!dot_fusable()) {
+        set_error("fused dot product needs the packed stencil with warp-aligned blocks");
+        return CVCB_ERR_STATE;
+      }
+      a.dotp = *dotp;
+      a.dot_part = dot_part;
+      a.dot_np = ((g.Vh + shape.bx - 1) / shape.bx) * (shape.bx / 32);
+      dot_np = a.dot_np;
+    }
     // FP64 sweeps of a reduced-precision solve (reliable updates) have their
     // own tuned shape; FP64 kernels keep one rhs per thread (register budget).
     LaunchShape sh = sizeof(typename AF::R) == 8 && sizeof(typename SF::R) != 8 ? shape64 : shape;
@@ -551,7 +579,7 @@ struct Batch {
     CVCB_LAUNCHED(L);
     if (rec_this) {
       CVCB_CUDA(cudaEventRecordWithFlags(rec.b, L->stream, capturing ? cudaEventRecordExternal : 0));
-      rec.bytes_per_rhs = (double)g.Vh * spinor_bytes<AF>() * (AUX ? 3 : 2);
+      rec.bytes_per_rhs = (double)g.Vh * spinor_bytes<AF>() * ((AUX ? 3 : 2) + (dot_part ? 1 : 0));
       rec.link_bytes = 4.0 * g.V * link_bytes<LL>();
       recs.push_back(rec);
     }
@@ -566,8 +594,15 @@ struct Batch {
     b = -m / d;
   }
 
-  // out_o = M^+ M in_o with sloppy fields (te, yo, te2 as intermediates)
-  int normal_op_sloppy(SF out, SF in, const int *done) {
+  // <p, Ap> in the last sweep of M^+M: the packed FP32x2 kernel with blocks
+  // a multiple of a warp wide
+  bool dot_fusable() const {
+    return sizeof(typename SF::R) == 4 && shape.pk == 1 && shape.bx % 32 == 0;
+  }
+
+  // out_o = M^+ M in_o with sloppy fields (te, yo, te2 as intermediates); with
+  // dot_part, per-warp partials of Re <in, out> as well
+  int normal_op_sloppy(SF out, SF in, const int *done, double *dot_part = nullptr) {
     double ia, ib, ja, jb;
     ainv(mu, ia, ib);
     ainv(-mu, ja, jb);
@@ -578,15 +613,21 @@ struct Batch {
     // K1': te2 = A^-1(-mu) (-1/2 H_eo g5 yo)
     CVCB_TRY((hop<SF, LF, true, false, false>(te2, yo, yo, links, 0, done, ja, jb, 0, 0, -0.5)));
     // K2': out = A(-mu) yo + 1/2 g5 H_oe te2
-    return hop<SF, LF, false, true, true>(out, te2, yo, links, 1, done, 1, 0, ka(), -mu, 0.5);
+    return hop<SF, LF, false, true, true>(out, te2, yo, links, 1, done, 1, 0, ka(), -mu, 0.5,
+                                          dot_part, &in);
   }
 
   // one CG iteration (sloppy)
   int iteration() {
-    CVCB_TRY(normal_op_sloppy(Ap, p, S.done));
     dim3 rg(red_blocks_sites(g.Vh), n);
-    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedPAp<SF>{p, Ap}, EpiAlphaB{S}, g.Vh, br,
-                                                    S.done);
+    if (dot_fusable()) {
+      CVCB_TRY(normal_op_sloppy(Ap, p, S.done, dot_part));
+      k_dot_finish<<<n, kRedThreads, 0, L->stream>>>(dot_part, dot_np, EpiAlphaB{S}, S.done);
+    } else {
+      CVCB_TRY(normal_op_sloppy(Ap, p, S.done));
+      k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedPAp<SF>{p, Ap}, EpiAlphaB{S}, g.Vh, br,
+                                                      S.done);
+    }
     CVCB_LAUNCHED(L);
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedUpdate<SF>{Ap, rs, S},
                                                     EpiBetaB{S}, g.Vh, br, S.done);
@@ -618,13 +659,16 @@ struct Batch {
   // and |r_hat|^2 in FP64 with the exact operator (the convergence criterion);
   // then the sloppy recursion restarts from r_s = M^+ r_hat, which only feeds
   // the sloppy iterations and is therefore formed in sloppy precision.
+  // absorb = false is the start from x = 0, where M x = 0 needs no sweep.
   int reliable_update(bool absorb) {
     dim3 eg((g.Vh + 127) / 128, n);
     if (absorb) {
       k_absorb<<<eg, 128, 0, L->stream>>>(f64(x64, 1), xs, S.scale, ru_skip, g.Vh, n);
       CVCB_LAUNCHED(L);
+      CVCB_TRY(schur64(y64, x64, mu, ru_skip));
+    } else {
+      CVCB_CUDA(cudaMemsetAsync(y64, 0, (size_t)12 * g.V * sizeof(double2) * n, L->stream));
     }
-    CVCB_TRY(schur64(y64, x64, mu, ru_skip));
     dim3 rg(red_blocks_sites(g.Vh), n);
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedRhat{f64(bh64, 1), f64(y64, 1)},
                                                     EpiRhat{S}, g.Vh, br, ru_skip);
@@ -722,7 +766,9 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   const size_t scal = 8 * rnd(sizeof(double) * kMaxBatch) + 3 * rnd(sizeof(int) * kMaxBatch);
   const size_t part = rnd(sizeof(double) * kMaxRedBlocks * kMaxBatch) +
                       rnd(sizeof(unsigned) * kMaxBatch);
-  const size_t total = 5 * rnd(f64) + 6 * (rnd(sl) + rnd(nrm)) + rnd(xsl) + rnd(nrm) + scal + part;
+  const size_t dotb = sizeof(double) * (size_t)n * (g.Vh / 32 + 64);
+  const size_t total = 5 * rnd(f64) + 6 * (rnd(sl) + rnd(nrm)) + rnd(xsl) + rnd(nrm) + scal + part +
+                       rnd(dotb);
   void *mem;
   CVCB_TRY(ensure_buffer(L, SLOT_MIX0, total, &mem));
   char *p = static_cast<char *>(mem);
@@ -762,6 +808,7 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   B.rst_skip = (int *)take(sizeof(int) * kMaxBatch);
   B.br.partials = (double *)take(sizeof(double) * kMaxRedBlocks * kMaxBatch);
   B.br.counters = (unsigned *)take(sizeof(unsigned) * kMaxBatch);
+  B.dot_part = (double *)take(dotb);
   CVCB_CUDA(cudaMemsetAsync(B.br.counters, 0, sizeof(unsigned) * kMaxBatch, L->stream));
   CVCB_CUDA(cudaMemsetAsync(B.S.done, 0, sizeof(int) * kMaxBatch, L->stream));
   CVCB_CUDA(cudaMemsetAsync(B.ru_skip, 0, sizeof(int) * kMaxBatch, L->stream));
