@@ -405,7 +405,8 @@ def main():
 def run_reference_arm(args, cb):
     """The reference's CPU solver on all usable host cores: one unmodified
     invert_Qtm_her per worker process on its own column; each step is a
-    bounded sample (two iterations per worker)."""
+    bounded sample (runs of one and two iterations per worker, whose
+    difference is the time of one iteration without the set-up)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bind as ob
     if not ob.reference_available():
@@ -417,7 +418,7 @@ def run_reference_arm(args, cb):
     n_conv = 89.0  # iterations of invert_Qtm_her for these columns (FP64 mirror on the GPU)
     times = []
     for i in range(args.warmup + args.steps):
-        sec_it, _ = reference_iteration_seconds(workers)
+        sec_it, _ = reference_iteration_seconds(workers, 1, 2)
         if i >= args.warmup:
             times.append(sec_it)
     sec_it = float(np.mean(times))
@@ -433,7 +434,7 @@ def run_reference_arm(args, cb):
                    "solver": "reference invert_Qtm_her (BiCGStab on Q^+Q), serial per process",
                    "processes": workers},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "reference",
-                         "sample": f"{workers} processes x 2 invert_Qtm_her iterations per step "
+                         "sample": f"{workers} processes x 1 + 2 invert_Qtm_her iterations per step "
                                    f"({sec_it:.2f} s/iteration), extrapolated to {n_conv:.0f} "
                                    f"iterations per solve; host has {cores} cores"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
