@@ -1313,9 +1313,19 @@ int solve_pipelined(cvcb_lattice *L, double *const *x, const double *const *b, i
     in[k] = static_cast<double *>(a);
     out[k] = static_cast<double *>(c);
   }
-  const int nbatch = (nrhs + nb - 1) / nb;
+  // Batches: a short first one (nb/3 rhs), so that the solve starts after a
+  // short upload, then full ones; the last takes the rest.  Only the first
+  // upload and the last download do not overlap a solve.
+  std::vector<int> boff, bn;
+  for (int off = 0; off < nrhs;) {
+    const int n = std::min(boff.empty() && nrhs > 2 * nb ? std::max(1, nb / 3) : nb, nrhs - off);
+    boff.push_back(off);
+    bn.push_back(n);
+    off += n;
+  }
+  const int nbatch = (int)boff.size();
   auto prefetch = [&](int k) -> int {
-    const int off = k * nb, n = std::min(nb, nrhs - off), s = k % 2;
+    const int off = boff[k], n = bn[k], s = k % 2;
     if (k >= 2) CVCB_CUDA(cudaStreamWaitEvent(cs, read[s], 0));
     for (int i = 0; i < n; ++i)
       CVCB_CUDA(cudaMemcpyAsync(in[s] + (size_t)i * fbytes / sizeof(double), b[off + i], fbytes,
@@ -1327,7 +1337,7 @@ int solve_pipelined(cvcb_lattice *L, double *const *x, const double *const *b, i
   std::vector<double *> xs(nb);
   std::vector<const double *> bs(nb);
   for (int k = 0; k < nbatch && rc >= 0; ++k) {
-    const int off = k * nb, n = std::min(nb, nrhs - off), s = k % 2;
+    const int off = boff[k], n = bn[k], s = k % 2;
     if (k + 1 < nbatch && (rc = prefetch(k + 1)) < 0) break;
     for (int i = 0; i < n; ++i) {
       bs[i] = in[s] + (size_t)i * fbytes / sizeof(double);

@@ -168,8 +168,10 @@ def test_batched_solver_tiny_magnitudes(cb, prec):
 def test_host_fields_pipeline_matches_device_fields(cb, env):
     """Host-resident fields over several batches take the copy/compute
     pipeline (sources of the next batch and solutions of the previous one
-    move on a second stream); the results equal those of device-resident
-    fields solved batch by batch."""
+    move on copy streams; the first batch is short).  Its batches are cut
+    differently from the device path's, which changes where each rhs's
+    reliable updates fall, so the two agree to the solver's accuracy: both
+    meet the 1e-10 residual, solutions compared at 1e-8 as elsewhere."""
     torch = pytest.importorskip("torch")
     lat, _, _ = env
     V = lat.VOLUME
@@ -186,4 +188,4 @@ def test_host_fields_pipeline_matches_device_fields(cb, env):
     torch.cuda.synchronize()
     assert st2.converged == n
     for a, d in zip(xh, xd):
-        assert rel_err(a, d.cpu().numpy()) < 1e-14
+        assert rel_err(a, d.cpu().numpy()) < 1e-8
