@@ -10,12 +10,13 @@
 //   CG on M^+ M x_o = b_N in sloppy precision (FP32 or FP16+norm spinors,
 //   12-real or 18-real links); every time the sloppy residual has fallen by
 //   `delta` (or the residual estimate reaches the target) the FP64 solution
-//   absorbs the sloppy one and the true residuals r_hat = b_hat - M x and
-//   r_N = M^+ r_hat are recomputed in FP64 with the exact 18-real operator.
+//   absorbs the sloppy one, the true residual r_hat = b_hat - M x is
+//   recomputed in FP64 with the exact 18-real operator, and the sloppy
+//   recursion restarts from r_N = M^+ r_hat (formed in sloppy precision).
 //   |r_hat| is the residual of the full system (the even rows vanish by
 //   construction), so convergence is decided on |b - Q x| / |b| in FP64.
-//   Finally x_e = A_ee^-1 (b_e + 1/2 H_eo x_o) and |b - Q x| is checked with
-//   the full-lattice FP64 operator.
+//   Finally x_e = A_ee^-1 (b_e + 1/2 H_eo x_o), Q x is recomputed in FP64 on
+//   both parities and |b - Q x| / |b| is checked.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
