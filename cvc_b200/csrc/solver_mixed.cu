@@ -914,7 +914,7 @@ int tune_shape64(cvcb_lattice *L, Batch<SF, XF, LF> &B) {
     return CVCB_OK;
   }
   const LaunchShape cands[] = {{64, 1, 1}, {128, 1, 1}, {32, 2, 1}, {64, 2, 1}, {32, 3, 1},
-                               {32, 4, 1}, {16, 4, 1}, {64, 3, 1}, {32, 6, 1}, {16, 6, 1}};
+                               {32, 4, 1}, {16, 4, 1}, {16, 8, 1}, {16, 6, 1}};
   LaunchShape best{64, 1, 1};
   float best_ms = 1e30f;
   for (const LaunchShape &c : cands) {
