@@ -581,8 +581,16 @@ __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_x2(HopArgs<SF, LF>
     for (int s = 0; s < 4; ++s)
 #pragma unroll
       for (int c = 0; c < 3; ++c) acc.c[s][c].re = acc.c[s][c].im = make_float2(0.f, 0.f);
+    // Directions in the order z, y, x, t: the z neighbours of a block's
+    // sites are its own index range of the other parity, and the y neighbours
+    // overlap it, so the loads of z+, y- and y+ find most of their lines in
+    // L1 right after z-.  1.085 ms per M^+M at 24^3x48, 12 rhs, against
+    // 1.129 ms in the order t, x, y, z, where the t and x loads evict the
+    // block's lines between the y and z loads.  (The FP64 staged sweep is
+    // slower in this order and keeps t, x, y, z.)
 #pragma unroll
-    for (int mu = 0; mu < 4; ++mu) {
+    for (int m = 0; m < 4; ++m) {
+      const int mu = 3 - m;
       {  // backward: (1 + g_mu) U_mu(x-mu)^+ in(x-mu)
         const int j = nb_lex(g, cd, mu, -1) >> 1;
         const Link<float> W = phased_link<float>(A.links, mu, qoff + j);
