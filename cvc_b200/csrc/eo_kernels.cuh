@@ -263,22 +263,21 @@ struct HopArgs {
   double d1a, d1b;  // D1 = d1a + i d1b g5
   double d2a, d2b;  // D2 = d2a + i d2b g5
   double c;         // hop coefficient
-  // optional (k_eo_hop_x2 only): per-warp partial sums of Re <dotp, out>,
+  // optional (k_eo_hop_x2 only): per-warp partial sums of |out|^2,
   // dot_part[rhs * dot_np + warp], warp = site block * (blockDim.x / 32) +
   // warp in the row; null = off
-  SF dotp;
   double *dot_part;
   int dot_np;
 };
 
-// Re <a, b> of two sites, accumulated in FP64
-__device__ __forceinline__ double redot_site(const Spinor<float> &a, const Spinor<float> &b) {
+// |a|^2 of one site, accumulated in FP64
+__device__ __forceinline__ double norm2_site(const Spinor<float> &a) {
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < 4; ++k)
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-      s += (double)a.c[k][c].re * b.c[k][c].re + (double)a.c[k][c].im * b.c[k][c].im;
+      s += (double)a.c[k][c].re * a.c[k][c].re + (double)a.c[k][c].im * a.c[k][c].im;
   return s;
 }
 
@@ -558,6 +557,8 @@ __device__ __forceinline__ void accum_recon_pair(int mu, int s, SpinorPair &acc,
 }
 
 // Packed-pair stencil: thread = (site, rhs pair); same sweep as k_eo_hop.
+// The aux term is loaded after the neighbours: starting the accumulator from
+// it instead (one load fewer at the end) measured 2.5 % slower in FP32.
 template <class SF, class LF, bool G5IN, bool G5HOP, bool AUX>
 __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_x2(HopArgs<SF, LF> A) {
   static_assert(sizeof(typename SF::R) == 4, "packed pairs need FP32 arithmetic");
@@ -573,7 +574,7 @@ __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_x2(HopArgs<SF, LF>
   const int qoff = (1 - p) * g.Vh;
   for (int sb = blockIdx.y; sb * (int)blockDim.x < g.Vh; sb += gridDim.y) {
     const int i = sb * blockDim.x + threadIdx.x;
-    double da = 0.0, db = 0.0;  // Re <dotp, out> of this site, rhs a and b
+    double da = 0.0, db = 0.0;  // |out|^2 of this site, rhs a and b
     if (i < g.Vh) {
     const SiteCoord cd = site_coord(g, p, i);
     SpinorPair acc;
@@ -638,7 +639,7 @@ __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_x2(HopArgs<SF, LF>
 #pragma unroll
           for (int q = 0; q < 3; ++q) o.c[s][q] = o.c[s][q] + x.c[s][q];
       }
-      if (A.dot_part) (lane == 0 ? da : db) = redot_site(A.dotp.load(r, i), o);
+      if (A.dot_part) (lane == 0 ? da : db) = norm2_site(o);
       A.out.store(r, i, o);
     }
     }  // i < Vh

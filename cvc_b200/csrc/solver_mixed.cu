@@ -115,7 +115,8 @@ struct Scal {  // per right-hand side, device arrays
   int *done;
 };
 
-// pAp = Re <p, Ap>; alpha = rr / pAp
+// pAp = Re <p, Ap>; alpha = rr / pAp (kernels other than the packed one;
+// the packed one takes pAp = |M p|^2 from the sweep that writes M p)
 template <class SF>
 struct RedPAp {
   SF p, Ap;
@@ -132,8 +133,8 @@ struct EpiAlphaB {
   }
 };
 
-// Sum of the per-warp partials of <p, Ap> that the last sweep of M^+M wrote
-// (fixed order: deterministic), then the epilogue (alpha).
+// Sum of the per-warp partials of <p, M^+M p> = |M p|^2 that the second
+// sweep of M^+M wrote (fixed order: deterministic), then the epilogue (alpha).
 template <class E>
 __global__ void __launch_bounds__(kRedThreads)
     k_dot_finish(const double *__restrict__ part, int np, E e, const int *__restrict__ skip) {
@@ -484,7 +485,9 @@ struct Batch {
   void *xs_mem;
   size_t xs_bytes;
   Scal S;
-  double *dot_part = nullptr;  // [rhs][dot_np] partials of <p, Ap> (fused into the stencil)
+  // [rhs][dot_np] partials of <p, M^+M p> = |M p|^2, fused into the sweep
+  // that produces M p
+  double *dot_part = nullptr;
   int dot_np = 0;
   int *ru_skip;   // per rhs: 1 = skip in the reliable update
   int *rst_skip;  // per rhs: 0 = restart the direction from the residual
@@ -508,17 +511,16 @@ struct Batch {
   F64Acc f64full(double2 *base) const { return F64Acc{base, (size_t)g.V, (size_t)12 * g.V}; }
 
   // With dot_part (packed kernel only, warp-aligned blocks), the sweep also
-  // writes per-warp partials of Re <dotp, out> (dot_np per rhs).
+  // writes per-warp partials of |out|^2 (dot_np per rhs).
   template <class AF, class LL, bool G5IN, bool G5HOP, bool AUX>
   int hop(AF out, AF in, AF aux, LL lk, int parity, const int *done, double d1a, double d1b,
-          double d2a, double d2b, double c, double *dot_part = nullptr, const AF *dotp = nullptr) {
+          double d2a, double d2b, double c, double *dot_part = nullptr) {
     HopArgs<AF, LL> a{out, in, aux, lk, EoGeom{g, parity}, n, done, d1a, d1b, d2a, d2b, c};
     if (dot_part) {
       if (!dot_fusable()) {
-        set_error("fused dot product needs the packed stencil with warp-aligned blocks");
+        set_error("fused norm needs the packed stencil with warp-aligned blocks");
         return CVCB_ERR_STATE;
       }
-      a.dotp = *dotp;
       a.dot_part = dot_part;
       a.dot_np = ((g.Vh + shape.bx - 1) / shape.bx) * (shape.bx / 32);
       dot_np = a.dot_np;
@@ -580,7 +582,7 @@ struct Batch {
     CVCB_LAUNCHED(L);
     if (rec_this) {
       CVCB_CUDA(cudaEventRecordWithFlags(rec.b, L->stream, capturing ? cudaEventRecordExternal : 0));
-      rec.bytes_per_rhs = (double)g.Vh * spinor_bytes<AF>() * ((AUX ? 3 : 2) + (dot_part ? 1 : 0));
+      rec.bytes_per_rhs = (double)g.Vh * spinor_bytes<AF>() * (AUX ? 3 : 2);
       rec.link_bytes = 4.0 * g.V * link_bytes<LL>();
       recs.push_back(rec);
     }
@@ -595,27 +597,28 @@ struct Batch {
     b = -m / d;
   }
 
-  // <p, Ap> in the last sweep of M^+M: the packed FP32x2 kernel with blocks
-  // a multiple of a warp wide
+  // <p, M^+M p> = |M p|^2 in the sweep that writes M p: the packed FP32x2
+  // kernel with blocks a multiple of a warp wide
   bool dot_fusable() const {
     return sizeof(typename SF::R) == 4 && shape.pk == 1 && shape.bx % 32 == 0;
   }
 
-  // out_o = M^+ M in_o with sloppy fields (te, yo, te2 as intermediates); with
-  // dot_part, per-warp partials of Re <in, out> as well
+  // out_o = M^+ M in_o with sloppy fields (te, yo, te2 as intermediates);
+  // with dot_part, per-warp partials of <in, M^+M in> = |M in|^2 as well,
+  // taken in the sweep that writes M in (no extra field read)
   int normal_op_sloppy(SF out, SF in, const int *done, double *dot_part = nullptr) {
     double ia, ib, ja, jb;
     ainv(mu, ia, ib);
     ainv(-mu, ja, jb);
     // K1: te = A^-1(mu) (-1/2 H_eo in)
     CVCB_TRY((hop<SF, LF, false, false, false>(te, in, in, links, 0, done, ia, ib, 0, 0, -0.5)));
-    // K2: yo = A(mu) in + 1/2 H_oe te
-    CVCB_TRY((hop<SF, LF, false, false, true>(yo, te, in, links, 1, done, 1, 0, ka(), mu, 0.5)));
+    // K2: yo = A(mu) in + 1/2 H_oe te  (= M in)
+    CVCB_TRY((hop<SF, LF, false, false, true>(yo, te, in, links, 1, done, 1, 0, ka(), mu, 0.5,
+                                              dot_part)));
     // K1': te2 = A^-1(-mu) (-1/2 H_eo g5 yo)
     CVCB_TRY((hop<SF, LF, true, false, false>(te2, yo, yo, links, 0, done, ja, jb, 0, 0, -0.5)));
     // K2': out = A(-mu) yo + 1/2 g5 H_oe te2
-    return hop<SF, LF, false, true, true>(out, te2, yo, links, 1, done, 1, 0, ka(), -mu, 0.5,
-                                          dot_part, &in);
+    return hop<SF, LF, false, true, true>(out, te2, yo, links, 1, done, 1, 0, ka(), -mu, 0.5);
   }
 
   // one CG iteration (sloppy)
@@ -1196,6 +1199,8 @@ int time_stencil_t(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int
   B.ainv(B.mu, ia, ib);
   auto one = [&] {
     if (kind == 2) return B.normal_op_sloppy(B.Ap, B.p, nullptr);
+    if (kind == 3)
+      return B.normal_op_sloppy(B.Ap, B.p, nullptr, B.dot_fusable() ? B.dot_part : nullptr);
     return B.template hop<SF, LF, false, false, false>(B.te, B.p, B.p, B.links, 0, nullptr, ia,
                                                        ib, 0, 0, -0.5);
   };
@@ -1222,7 +1227,7 @@ int time_stencil(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int r
     set_error("no gauge field uploaded");
     return CVCB_ERR_STATE;
   }
-  if (reps <= 0 || nrhs <= 0 || nrhs > kMaxBatch) return CVCB_ERR_ARG;
+  if (reps <= 0 || nrhs <= 0 || nrhs > kMaxBatch || kind < 0 || kind > 3) return CVCB_ERR_ARG;
   if (kind == 0) {
     const size_t fb = (size_t)L->g.V * 12 * sizeof(double2);
     void *f0, *f1;

@@ -4,7 +4,8 @@
 
 kind 0: Q_phi_tbc on one FP64 field (all V sites); kind 1: one half-lattice
 sweep of the batched solver's stencil; kind 2: one application of its normal
-operator M^+ M (four sweeps).  The lattice and gauge field are those of the
+operator M^+ M (four sweeps); kind 3: the same with the fused partial sums of
+|M p|^2 of a CG iteration (no extra field traffic).  The lattice and gauge field are those of the
 solver benchmark (24^3x48, ranlxd seed 11, eps 0.25) unless overridden.
 Prints one line: milliseconds per call and algorithmic GB/s.
 """
@@ -26,12 +27,12 @@ def algorithmic_bytes(kind, prec, recon, nrhs, dims):
         return V * (2 * 192 + 8 * 144)      # spinor in/out + 8 links per site (FP64)
     links = 4 * V * _LINK[(prec, 18 if prec == 0 else recon)]
     sweep = lambda nf: nrhs * Vh * nf * _SPINOR[prec] + links
-    return sweep(2) if kind == 1 else 2 * sweep(2) + 2 * sweep(3)
+    return sweep(2) if kind == 1 else 2 * sweep(2) + 2 * sweep(3)  # kinds 2 and 3
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--kind", type=int, default=1, choices=(0, 1, 2))
+    ap.add_argument("--kind", type=int, default=1, choices=(0, 1, 2, 3))
     ap.add_argument("--precision", default="single", choices=tuple(_PREC))
     ap.add_argument("--recon", type=int, default=12, choices=(12, 18))
     ap.add_argument("--nrhs", type=int, default=12)

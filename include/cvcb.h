@@ -245,7 +245,8 @@ int cvcb_solve(cvcb_lattice *lat, double *const *x, const double *const *b, int 
  * the batched solver's stencil (V/2 output sites) for nrhs right-hand sides
  * in the given precision and link format, with the autotuned launch shape;
  * kind 2: one application of the solver's normal operator M^+ M (four such
- * sweeps), reported per application.
+ * sweeps), reported per application; kind 3: the same with the partial sums
+ * of |M p|^2 that a CG iteration takes along (where the kernel fuses them).
  * Field contents are zero (timing does not depend on them). */
 int cvcb_time_stencil(cvcb_lattice *lat, int kind, int precision, int link_recon, int nrhs,
                       int reps, double *ms_per_launch);
