@@ -192,6 +192,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true",
                     help="skip the plain FP64 GPU solver comparison")
+    ap.add_argument("--block-rhs", type=int, default=0,
+                    help="rhs per batch (0: autotuned); pins the batch for profiling runs, "
+                         "whose timings would mislead the tuner")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -225,6 +228,7 @@ def main():
     params = cb.solver_defaults()
     params.precision, params.tol = prec, TOL
     params.link_recon = 18 if prec == cb.PREC_DOUBLE else 12
+    params.block_rhs = args.block_rhs
 
     # device-resident inputs (point sources) and outputs
     dev = torch.device("cuda", local)

@@ -110,6 +110,8 @@ def test_stencil_timing_algorithmic_bytes():
     dims = (48, 24, 24, 24)
     assert algorithmic_bytes(1, 1, 12, 12, dims) == 891_813_888
     assert algorithmic_bytes(2, 1, 12, 12, dims) == 2 * 891_813_888 + 2 * 1_274_019_840
+    # the fused |M p|^2 of a CG iteration reads no field: same bytes as M^+M alone
+    assert algorithmic_bytes(3, 1, 12, 12, dims) == algorithmic_bytes(2, 1, 12, 12, dims)
     assert algorithmic_bytes(0, 0, 18, 1, dims) == 663_552 * (2 * 192 + 8 * 144)
 
 
