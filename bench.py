@@ -39,6 +39,9 @@ KAPPA = 0.155
 MU = 0.005 / (2 * KAPPA)
 EPS, SEED = 0.25, 11
 NSRC, TOL = 8, 1e-10
+WORKLOAD = ("24^3x48 twisted-mass Wilson, kappa 0.155, 2*kappa*mu 0.005, eps 0.25 gauge "
+            "(ranlxd seed 11), 8 point sources x 12 spin-colour = 96 rhs per GPU, "
+            "true FP64 residual <= 1e-10")
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -305,9 +308,7 @@ def main():
         "dtype": {"single": "f32", "half": "f16-storage/f32", "double": "f64"}[args.precision],
         "data": "synthetic",
         "config": {
-            "workload": "24^3x48 twisted-mass Wilson, kappa 0.155, 2*kappa*mu 0.005, "
-                        "eps 0.25 gauge (ranlxd seed 11), 8 point sources x 12 spin-colour "
-                        "= 96 rhs per GPU, true FP64 residual <= 1e-10",
+            "workload": WORKLOAD,
             "lattice": list(DIMS), "rhs_per_gpu": nrhs, "solver": "even/odd CG on M^+M, "
             f"{args.precision} inner iterations, FP64 reliable updates, batched",
             "link_recon": params.link_recon, "parallelism": f"rhs-sharded x{world}",
@@ -433,8 +434,7 @@ def run_reference_arm(args, cb):
         "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": sec_it * 2e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "24^3x48 twisted-mass Wilson, kappa 0.155, 2*kappa*mu 0.005, "
-                               "eps 0.25 gauge (ranlxd seed 11), point-source columns",
+        "config": {"workload": WORKLOAD, "lattice": list(DIMS),
                    "solver": "reference invert_Qtm_her (BiCGStab on Q^+Q), serial per process",
                    "processes": workers},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "reference",
