@@ -7,7 +7,11 @@ sweep of the batched solver's stencil; kind 2: one application of its normal
 operator M^+ M (four sweeps); kind 3: the same with the fused partial sums of
 |M p|^2 of a CG iteration (no extra field traffic).  The lattice and gauge field are those of the
 solver benchmark (24^3x48, ranlxd seed 11, eps 0.25) unless overridden.
-Prints one line: milliseconds per call and algorithmic GB/s.
+Prints one line: milliseconds per call, algorithmic GB/s (compulsory traffic:
+each input spinor, output spinor and link once) and, labelled, the no-reuse
+figure (every one of the 8 neighbour spinors and 8 links of a site counted at
+each use, links once per rhs pair of the packed kernel), which counts what the
+caches serve and can exceed the HBM peak.
 """
 import argparse
 import ctypes
@@ -24,10 +28,27 @@ def algorithmic_bytes(kind, prec, recon, nrhs, dims):
     V = T * LX * LY * LZ
     Vh = V // 2
     if kind == 0:
-        return V * (2 * 192 + 8 * 144)      # spinor in/out + 8 links per site (FP64)
+        # spinor in and out, and the 4 links of the site (each link serves the
+        # forward hop of its site and the backward hop of its neighbour)
+        return V * (2 * 192 + 4 * 144)
     links = 4 * V * _LINK[(prec, 18 if prec == 0 else recon)]
     sweep = lambda nf: nrhs * Vh * nf * _SPINOR[prec] + links
     return sweep(2) if kind == 1 else 2 * sweep(2) + 2 * sweep(3)  # kinds 2 and 3
+
+
+def no_reuse_bytes(kind, prec, recon, nrhs, dims, rhs_per_link=2):
+    """8 neighbour spinors + 8 links + output (+ the diagonal term's input)
+    per output site and rhs, links shared by `rhs_per_link` rhs (FP64
+    full-lattice operator: 8 x 192 + 8 x 144 + 192 + 192 = 3072 B per site)."""
+    T, LX, LY, LZ = dims
+    V = T * LX * LY * LZ
+    if kind == 0:
+        return V * (8 * 192 + 8 * 144 + 2 * 192)
+    s = _SPINOR[prec]
+    r = _LINK[(prec, 18 if prec == 0 else recon)]
+    per = lambda aux: 8 * s + 8 * r / rhs_per_link + s * (1 + aux)
+    sweep = lambda aux: nrhs * (V // 2) * per(aux)
+    return sweep(0) if kind == 1 else 2 * sweep(0) + 2 * sweep(1)
 
 
 def main(argv=None):
@@ -48,8 +69,10 @@ def main(argv=None):
     _lat._check("cvcb_time_stencil", lat._lib.cvcb_time_stencil(
         lat._h, a.kind, prec, a.recon, a.nrhs, a.reps, ctypes.byref(ms)))
     nbytes = algorithmic_bytes(a.kind, prec, a.recon, a.nrhs, a.dims)
+    nr = no_reuse_bytes(a.kind, prec, a.recon, a.nrhs, a.dims)
     print(f"kind {a.kind} {a.precision} recon {a.recon} nrhs {a.nrhs} dims {list(a.dims)}: "
-          f"{ms.value:.4f} ms per call, {nbytes / ms.value / 1e6:.1f} GB/s algorithmic")
+          f"{ms.value:.4f} ms per call, {nbytes / ms.value / 1e6:.1f} GB/s algorithmic "
+          f"({nr / ms.value / 1e6:.1f} GB/s no-reuse)")
     lat.close()
 
 

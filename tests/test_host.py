@@ -112,7 +112,13 @@ def test_stencil_timing_algorithmic_bytes():
     assert algorithmic_bytes(2, 1, 12, 12, dims) == 2 * 891_813_888 + 2 * 1_274_019_840
     # the fused |M p|^2 of a CG iteration reads no field: same bytes as M^+M alone
     assert algorithmic_bytes(3, 1, 12, 12, dims) == algorithmic_bytes(2, 1, 12, 12, dims)
-    assert algorithmic_bytes(0, 0, 18, 1, dims) == 663_552 * (2 * 192 + 8 * 144)
+    assert algorithmic_bytes(0, 0, 18, 1, dims) == 663_552 * 960
+    # no-reuse counts: 3072 B per site for the FP64 operator; the packed FP32 sweep
+    # reads 8 x 96 + 8 x 48 / 2 + 96 (+ 96 with the diagonal term) per site and rhs
+    from cvc_b200.stencil_timing import no_reuse_bytes
+    assert no_reuse_bytes(0, 0, 18, 1, dims) == 663_552 * 3072
+    assert no_reuse_bytes(1, 1, 12, 12, dims) == 12 * 331_776 * 1056
+    assert no_reuse_bytes(2, 1, 12, 12, dims) == 12 * 331_776 * (2 * 1056 + 2 * 1152)
 
 
 def test_tmlqcd_library_exports_the_wrapper_abi(cb):
