@@ -11,7 +11,9 @@ Prints one line: milliseconds per call, algorithmic GB/s (compulsory traffic:
 each input spinor, output spinor and link once) and, labelled, the no-reuse
 figure (every one of the 8 neighbour spinors and 8 links of a site counted at
 each use, links once per rhs pair of the packed kernel), which counts what the
-caches serve and can exceed the HBM peak.
+caches serve and can exceed the HBM peak; and the flop rate in the Wilson
+convention (1320 flop per site for the hopping term, 48 for the diagonal
+term, 24 for the factor -1/2: 1392 per output site and rhs).
 """
 import argparse
 import ctypes
@@ -34,6 +36,19 @@ def algorithmic_bytes(kind, prec, recon, nrhs, dims):
     links = 4 * V * _LINK[(prec, 18 if prec == 0 else recon)]
     sweep = lambda nf: nrhs * Vh * nf * _SPINOR[prec] + links
     return sweep(2) if kind == 1 else 2 * sweep(2) + 2 * sweep(3)  # kinds 2 and 3
+
+
+FLOP_PER_SITE = 1320 + 48 + 24
+
+
+def flops(kind, nrhs, dims):
+    """Wilson-convention flops of one call: 1392 per output site and rhs and sweep."""
+    T, LX, LY, LZ = dims
+    V = T * LX * LY * LZ
+    if kind == 0:
+        return V * FLOP_PER_SITE
+    sweep = nrhs * (V // 2) * FLOP_PER_SITE
+    return sweep if kind == 1 else 4 * sweep
 
 
 def no_reuse_bytes(kind, prec, recon, nrhs, dims, rhs_per_link=2):
@@ -72,7 +87,8 @@ def main(argv=None):
     nr = no_reuse_bytes(a.kind, prec, a.recon, a.nrhs, a.dims)
     print(f"kind {a.kind} {a.precision} recon {a.recon} nrhs {a.nrhs} dims {list(a.dims)}: "
           f"{ms.value:.4f} ms per call, {nbytes / ms.value / 1e6:.1f} GB/s algorithmic "
-          f"({nr / ms.value / 1e6:.1f} GB/s no-reuse)")
+          f"({nr / ms.value / 1e6:.1f} GB/s no-reuse), "
+          f"{flops(a.kind, a.nrhs, a.dims) / ms.value / 1e9:.2f} TFLOP/s")
     lat.close()
 
 

@@ -115,7 +115,8 @@ def test_stencil_timing_algorithmic_bytes():
     assert algorithmic_bytes(0, 0, 18, 1, dims) == 663_552 * 960
     # no-reuse counts: 3072 B per site for the FP64 operator; the packed FP32 sweep
     # reads 8 x 96 + 8 x 48 / 2 + 96 (+ 96 with the diagonal term) per site and rhs
-    from cvc_b200.stencil_timing import no_reuse_bytes
+    from cvc_b200.stencil_timing import flops, no_reuse_bytes
+    assert flops(2, 12, dims) == 4 * 12 * 331_776 * 1392 and flops(0, 1, dims) == 663_552 * 1392
     assert no_reuse_bytes(0, 0, 18, 1, dims) == 663_552 * 3072
     assert no_reuse_bytes(1, 1, 12, 12, dims) == 12 * 331_776 * 1056
     assert no_reuse_bytes(2, 1, 12, 12, dims) == 12 * 331_776 * (2 * 1056 + 2 * 1152)
