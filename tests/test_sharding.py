@@ -1,5 +1,6 @@
-"""The multi-rank path on CPU: two gloo ranks shard source positions and
-gather Pi_mu_nu; the result must equal the single-process run bit for bit.
+"""The multi-rank path on CPU: two and three gloo ranks shard source positions
+(5 of them: uneven shares) and gather Pi_mu_nu; the result must equal the
+single-process run bit for bit.
 The per-source computation here is the oracle's contraction on a small
 lattice (the CUDA library is not needed to test the host orchestration)."""
 import os
@@ -63,11 +64,12 @@ def test_partition_covers_each_item_once():
         assert sorted(seen) == list(range(13))
 
 
-def test_two_gloo_ranks_match_single_process(oracle_mod):
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_match_single_process(oracle_mod, world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = [q.get(timeout=240) for _ in procs]
@@ -76,10 +78,10 @@ def test_two_gloo_ranks_match_single_process(oracle_mod):
         assert p.exitcode == 0
     serial = {s: pi_for_source(s) for s in SOURCES}
     for rank, res, stacked, tmax, mine in out:
-        assert tmax == 2.0
+        assert tmax == float(world)
         assert set(res) == set(SOURCES)
         for s in SOURCES:
             assert np.array_equal(res[s], serial[s])
         for i, s in enumerate(SOURCES):
             assert np.array_equal(stacked[i], serial[s])
-    assert sorted(out[0][4] + out[1][4]) == list(range(len(SOURCES)))
+    assert sorted(sum((o[4] for o in out), [])) == list(range(len(SOURCES)))
