@@ -378,6 +378,10 @@ int cvcb_gamma_tables(int *perm, int *sign) {
 
 int cvcb_boundary_phases(int T, int LX, int LY, int LZ, const double bc[4], double ph[8]) {
   if (!bc || !ph) return CVCB_ERR_NULL;
+  if (T <= 0 || LX <= 0 || LY <= 0 || LZ <= 0) {
+    set_error("boundary phases: extents %d x %d x %d x %d", T, LX, LY, LZ);
+    return CVCB_ERR_ARG;
+  }
   boundary_phases(T, LX, LY, LZ, bc, ph);
   return CVCB_OK;
 }

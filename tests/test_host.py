@@ -134,3 +134,25 @@ def test_tmlqcd_library_exports_the_wrapper_abi(cb):
     assert len(names) == 7
     for n in names:
         assert hasattr(lib, n), n
+
+
+def test_host_api_error_convention(cb):
+    """Host-only calls return the status codes of include/cvcb.h and set the
+    thread's error text; none of them needs a device."""
+    from cvc_b200 import _lib
+    lib = _lib.load()
+    perm = np.zeros(16 * 24, np.int32)
+    assert lib.cvcb_gamma_tables(None, perm.ctypes.data) == _lib.CVCB_ERR_NULL
+    ph = np.zeros(8)
+    bc = np.array([1.0, 0.0, 0.0, 0.0])
+    assert lib.cvcb_boundary_phases(8, 4, 4, 4, None, ph.ctypes.data) == _lib.CVCB_ERR_NULL
+    assert lib.cvcb_boundary_phases(8, 0, 4, 4, bc.ctypes.data, ph.ctypes.data) == _lib.CVCB_ERR_ARG
+    assert "extents" in cb.last_error()
+    assert lib.cvcb_geometry_tables(0, 4, 4, 4, *([None] * 9)) == _lib.CVCB_ERR_ARG
+    r = np.zeros(4)
+    assert lib.cvcb_ranlxd(3, 1, r.ctypes.data, 4) == _lib.CVCB_ERR_ARG     # level 1 or 2
+    assert lib.cvcb_ranlxd(1, 0, r.ctypes.data, 4) == _lib.CVCB_ERR_ARG     # seed > 0
+    assert lib.cvcb_gauge_random(None, 2, 2, 2, 2, 0.3, 1) == _lib.CVCB_ERR_ARG
+    out = ctypes.c_uint32()
+    assert lib.cvcb_crc32(0, None, 4, ctypes.byref(out)) == _lib.CVCB_ERR_NULL
+    assert lib.cvcb_crc32(0, None, 0, ctypes.byref(out)) == _lib.CVCB_OK and out.value == 0
