@@ -181,3 +181,25 @@ def test_contraction_files(cb, tmp_path):
     lime.write_lime_contraction(fn, conn, DIMS, 32)
     c32, _ = lime.read_lime_contraction(fn, DIMS, 16, 0)
     assert np.array_equal(c32, conn.astype(np.float32).astype(np.float64))
+
+
+def test_gauge_read_errors(cb, tmp_path):
+    """Wrong lattice, a truncated record and a file that is not LIME are
+    errors with a message, never a partial field."""
+    from cvc_b200 import lime
+    g = cb.gauge_random(*DIMS, 0.3, 5)
+    fn = tmp_path / "conf.0001"
+    lime.write_lime_gauge_field(fn, g, DIMS)
+    with pytest.raises(cb.CvcbError):
+        lime.read_lime_gauge_field(fn, (T, LX, LY, LZ + 2))
+    data = fn.read_bytes()
+    cut = tmp_path / "conf.cut"
+    cut.write_bytes(data[:len(data) // 2])
+    with pytest.raises(cb.CvcbError):
+        lime.read_lime_gauge_field(cut, DIMS)
+    junk = tmp_path / "conf.txt"
+    junk.write_bytes(b"plain text, not a LIME file\n" * 8)
+    with pytest.raises(cb.CvcbError, match="not a LIME file"):
+        lime.read_lime_gauge_field(junk, DIMS)
+    with pytest.raises(cb.CvcbError, match="cannot open"):
+        lime.read_lime_gauge_field(tmp_path / "missing", DIMS)
