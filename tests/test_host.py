@@ -156,3 +156,32 @@ def test_host_api_error_convention(cb):
     out = ctypes.c_uint32()
     assert lib.cvcb_crc32(0, None, 4, ctypes.byref(out)) == _lib.CVCB_ERR_NULL
     assert lib.cvcb_crc32(0, None, 0, ctypes.byref(out)) == _lib.CVCB_OK and out.value == 0
+
+
+def test_tmlqcd_wrapper_before_and_without_init(cb, tmp_path):
+    """The tmLQCD wrapper's status codes on the paths that touch no device:
+    every call before tmLQCD_invert_init is refused with 1, and init fails
+    with 1 on a missing input file or one without the lattice extents
+    (tmLQCD.h:46-54 of the reference; no exit() inside the library)."""
+    from cvc_b200 import _lib
+    lib = ctypes.CDLL(os.path.join(os.path.dirname(_lib.LIB_PATH), "libcvcb200_tmlqcd.so"))
+    assert lib.tmLQCD_finalise() == 0
+    buf = (ctypes.c_double * 24)()
+    assert lib.tmLQCD_invert(buf, buf, 0, 0) == 1
+    assert lib.tmLQCD_read_gauge(0) == 1
+    gf = ctypes.c_void_p()
+    assert lib.tmLQCD_get_gauge_field_pointer(ctypes.byref(gf)) == 1
+    params = (ctypes.c_uint * 16)()
+    assert lib.tmLQCD_get_lat_params(params) == 1
+    assert lib.tmLQCD_get_mpi_params(params) == 1
+
+    def init(path):
+        argv = (ctypes.c_char_p * 3)(b"prog", b"-f", str(path).encode())
+        return lib.tmLQCD_invert_init(3, argv, 0)
+
+    assert init(tmp_path / "missing.input") == 1
+    no_extents = tmp_path / "invert.input"
+    no_extents.write_text("# no T or L\nkappa = 0.15\n2KappaMu = 0.01\n")
+    assert init(no_extents) == 1
+    assert lib.tmLQCD_read_gauge(0) == 1     # still not initialised
+    assert lib.tmLQCD_finalise() == 0
