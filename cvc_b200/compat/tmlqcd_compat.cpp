@@ -132,6 +132,10 @@ int read_input(const char *name) {
     }
   }
   std::fclose(f);
+  if (in_block) {
+    std::fprintf(stderr, "[tmLQCD_invert_init] BeginOperator without EndOperator in %s\n", name);
+    return 2;
+  }
   g.ops.clear();
   for (const auto &b : blocks) {
     Operator op = defaults;

@@ -161,7 +161,8 @@ def test_host_api_error_convention(cb):
 def test_tmlqcd_wrapper_before_and_without_init(cb, tmp_path):
     """The tmLQCD wrapper's status codes on the paths that touch no device:
     every call before tmLQCD_invert_init is refused with 1, and init fails
-    with 1 on a missing input file or one without the lattice extents
+    with 1 on a missing input file, one without the lattice extents or one
+    with an operator block that is not closed
     (tmLQCD.h:46-54 of the reference; no exit() inside the library)."""
     from cvc_b200 import _lib
     lib = ctypes.CDLL(os.path.join(os.path.dirname(_lib.LIB_PATH), "libcvcb200_tmlqcd.so"))
@@ -183,5 +184,8 @@ def test_tmlqcd_wrapper_before_and_without_init(cb, tmp_path):
     no_extents = tmp_path / "invert.input"
     no_extents.write_text("# no T or L\nkappa = 0.15\n2KappaMu = 0.01\n")
     assert init(no_extents) == 1
+    open_block = tmp_path / "open.input"
+    open_block.write_text("T = 8\nL = 4\nBeginOperator TMWILSON\n  kappa = 0.15\n")
+    assert init(open_block) == 1
     assert lib.tmLQCD_read_gauge(0) == 1     # still not initialised
     assert lib.tmLQCD_finalise() == 0
