@@ -54,9 +54,11 @@ def measured_hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def source_sites(rank, cb):
+def source_sites(rank, ranlxd):
+    """Lexicographic indices of the rank's point sources; `ranlxd(n, seed)`
+    is the library's generator or the reference's own (the same stream)."""
     T, LX, LY, LZ = DIMS
-    r = cb.ranlxd(4 * NSRC, SEED + 1000 * rank)
+    r = ranlxd(4 * NSRC, SEED + 1000 * rank)
     sites = []
     for k in range(NSRC):
         t, x, y, z = (int(r[4 * k] * T), int(r[4 * k + 1] * LX), int(r[4 * k + 2] * LY),
@@ -130,40 +132,123 @@ def stencil_traffic_from_profile(key):
 
 
 # ---------------------------------------------------------------------------
-# reference arm: the reference's own CPU solver (oracle/_ref)
+# The reference's own CPU solver (oracle/_ref), for the reference arm and the
+# cpu_baseline leg.  Its inputs are built without the CUDA library: the gauge
+# field by the numpy restatement of the recipe (oracle/gauge_recipe.py) over
+# the reference's own ranlxd, the source positions from the same stream as
+# the GPU arm's.
 # ---------------------------------------------------------------------------
-def _ref_worker(args):
-    col, niters, q = args
+def _ref_worker(gauge_path, cmd_q, res_q, wid):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bind as ob
-    import cvc_b200 as cb
     ref = ob.Reference(*DIMS, KAPPA, MU)
-    ref.set_gauge(cb.gauge_random(*DIMS, EPS, SEED))
+    ref.set_gauge(np.load(gauge_path))
     V = ref.V
-    b = np.zeros(24 * V)
-    b[2 * (col % 12)] = 1.0
-    out = []
-    for n in niters:
+    res_q.put((wid, "ready", 0.0))
+    while True:
+        cmd = cmd_q.get()
+        if cmd is None:
+            return
+        site, sc, nmax = cmd
+        b = np.zeros(24 * V)
+        b[24 * site + 2 * sc] = 1.0
         t = time.perf_counter()
-        ref.invert(b, 1e-20, n - 1, her=True)  # runs n BiCGStab iterations (no convergence)
-        out.append(time.perf_counter() - t)
-    q.put(out)
+        rc, _ = ref.invert(b, TOL * TOL, nmax, her=True)
+        res_q.put((wid, rc, time.perf_counter() - t))
 
 
-def reference_iteration_seconds(workers, n_lo=1, n_hi=3):
-    """Seconds per invert_Qtm_her iteration per worker process, from two
-    bounded runs (n_lo and n_hi iterations) so that set-up cost cancels."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    procs = [ctx.Process(target=_ref_worker, args=((w, [n_lo, n_hi], q),)) for w in range(workers)]
-    for p in procs:
-        p.start()
-    res = [q.get() for _ in procs]
-    for p in procs:
-        p.join()
-    per = [(r[1] - r[0]) / (n_hi - n_lo) for r in res]
-    return max(per), per
+class ReferencePool:
+    """`workers` processes, each holding one unmodified reference instance
+    (its globals: one lattice per process) on the benchmark's gauge field.
+    Started with the spawn method, before any GPU work of this process."""
+
+    def __init__(self, workers):
+        import multiprocessing as mp
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_bind as ob
+        import gauge_recipe
+        self.workers = workers
+        self.sites = source_sites(0, ob.reference_ranlxd)
+        gauge = gauge_recipe.gauge_random(*DIMS, EPS, SEED, ob.reference_ranlxd)
+        self.tmp = tempfile.NamedTemporaryFile(suffix=".npy", delete=False)
+        np.save(self.tmp, gauge)
+        self.tmp.close()
+        del gauge
+        ctx = mp.get_context("spawn")
+        self.res = ctx.Queue()
+        self.cmds = [ctx.Queue() for _ in range(workers)]
+        self.procs = [ctx.Process(target=_ref_worker, args=(self.tmp.name, self.cmds[w], self.res, w))
+                      for w in range(workers)]
+        for p in self.procs:
+            p.start()
+        for _ in range(workers):
+            self.res.get()
+        os.unlink(self.tmp.name)
+
+    def column(self, w):
+        """Worker w's column: source position w // 12 (mod the 8), spin-colour w % 12."""
+        return self.sites[(w // 12) % NSRC], w % 12
+
+    def run(self, nmax):
+        """Every worker runs invert_Qtm_her on its own column with niter_max =
+        nmax; returns (wall seconds of the whole round, [(rc, seconds)])."""
+        t = time.perf_counter()
+        for w in range(self.workers):
+            self.cmds[w].put((*self.column(w), nmax))
+        out = [None] * self.workers
+        for _ in range(self.workers):
+            w, rc, dt = self.res.get()
+            out[w] = (rc, dt)
+        return time.perf_counter() - t, out
+
+    def close(self):
+        for q in self.cmds:
+            q.put(None)
+        for p in self.procs:
+            p.join()
+
+
+def reference_rate(pool, warmup, steps, n_conv=None):
+    """Reference solves/s on the pool.  The iteration count to convergence
+    is measured (every worker solves its column to the benchmark's residual)
+    unless given.  A run with niter_max = n costs (n + 1 + c) iterations,
+    c the fixed part (the initial residual and the final Qf5); c comes from
+    runs of 1 and 3 iterations, after which each step is one bounded round
+    of 2 iterations per worker."""
+    full = None
+    if n_conv is None:
+        wall, res = pool.run(20000)
+        its = [rc for rc, _ in res]
+        if min(its) < 0:
+            raise RuntimeError(f"reference solve did not converge: {its}")
+        n_conv = float(np.mean(its))
+        full = {"iterations": its, "wall_s": wall,
+                "solves_per_s": pool.workers / max(dt for _, dt in res)}
+    _, r1 = pool.run(0)
+    _, r3 = pool.run(2)
+    t1 = max(dt for _, dt in r1)
+    t3 = max(dt for _, dt in r3)
+    t_it = (t3 - t1) / 2
+    c = max(t1 / t_it - 1.0, 0.0)
+    times, walls = [], []
+    for i in range(warmup + steps):
+        wall, r = pool.run(1)
+        if i >= warmup:
+            times.append(max(dt for _, dt in r) / (2.0 + c))
+            walls.append(wall)
+    sec_it = float(np.mean(times))
+    return {"value": pool.workers / (sec_it * n_conv), "sec_per_iteration": sec_it,
+            "n_conv": n_conv, "fixed_iterations": c, "step_wall_s": walls, "full": full}
+
+
+def workload_config(world):
+    """The workload, identical in both arms (implementation details go
+    elsewhere in the line)."""
+    return {"workload": WORKLOAD, "lattice": list(DIMS), "kappa": KAPPA, "two_kappa_mu": 0.005,
+            "gauge": {"eps": EPS, "seed": SEED}, "rhs_per_gpu": NSRC * 12,
+            "true_residual": TOL, "parallelism": f"rhs-sharded x{world}",
+            "l2": "inputs larger than L2 (96 x 127 MB fields)"}
 
 
 def host_cores():
@@ -195,6 +280,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true",
                     help="skip the plain FP64 GPU solver comparison")
+    ap.add_argument("--ref-niter", type=int, default=0,
+                    help="reference arm: iterations per solve given instead of measured "
+                         "(0: measured by solving every worker's column first)")
     ap.add_argument("--block-rhs", type=int, default=0,
                     help="rhs per batch (0: autotuned); pins the batch for profiling runs, "
                          "whose timings would mislead the tuner")
@@ -204,13 +292,13 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
-    import cvc_b200 as cb
-
     if args.impl == "reference":
         if rank != 0:
             return 0
-        run_reference_arm(args, cb)
+        run_reference_arm(args)
         return 0
+
+    import cvc_b200 as cb
 
     import torch
     import torch.distributed as dist
@@ -225,7 +313,7 @@ def main():
     gauge = cb.gauge_random(*DIMS, EPS, SEED)
     lat.upload_gauge(gauge)
     V = lat.VOLUME
-    sites = source_sites(rank, cb)
+    sites = source_sites(rank, cb.ranlxd)
     nrhs = NSRC * 12
     prec = {"single": cb.PREC_SINGLE, "half": cb.PREC_HALF, "double": cb.PREC_DOUBLE}[args.precision]
     params = cb.solver_defaults()
@@ -307,13 +395,11 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"single": "f32", "half": "f16-storage/f32", "double": "f64"}[args.precision],
         "data": "synthetic",
-        "config": {
-            "workload": WORKLOAD,
-            "lattice": list(DIMS), "rhs_per_gpu": nrhs, "solver": "even/odd CG on M^+M, "
+        "config": workload_config(world),
+        "run": {
+            "solver": "even/odd CG on M^+M, "
             f"{args.precision} inner iterations, FP64 reliable updates, batched",
-            "link_recon": params.link_recon, "parallelism": f"rhs-sharded x{world}",
-            "l2": "inputs larger than L2 (96 x 127 MB fields)",
-            "rhs_per_batch": nb,
+            "link_recon": params.link_recon, "rhs_per_batch": nb,
             "stencil_shape": {"sites_per_block": shape[0].value, "rows_per_block": shape[1].value,
                               "rhs_per_thread": shape[2].value,
                               "variant": ["per-thread links", "shared-memory links",
@@ -382,22 +468,9 @@ def main():
                                  "transforms inside the timed region"}
         del pin_b, pin_x
 
-    # CPU baseline: the reference's own solver, serial, bounded sample
+    # CPU baseline: the reference's own solver on one host core, bounded sample
     if rank == 0 and world == 1 and not args.no_cpu:
-        try:
-            ref_its = result.get("fp64_plain_gpu", {}).get("iterations", [90])
-            n_conv = float(np.mean(ref_its))
-            sec_it, _ = reference_iteration_seconds(1)
-            result["cpu_baseline"] = {
-                "value": 1.0 / (sec_it * n_conv), "unit": "solves/s", "cores": 1,
-                "kind": "reference",
-                "sample": f"2 invert_Qtm_her iterations of the unmodified reference (serial, "
-                          f"oracle/_ref) on one 24^3x48 point-source column: {sec_it:.2f} s per "
-                          f"iteration, extrapolated to {n_conv:.0f} iterations per solve "
-                          "(the count the same algorithm needs on the GPU)"}
-        except Exception as e:  # the reference build is absent
-            result["cpu_baseline"] = {"value": None, "unit": "solves/s", "cores": 0,
-                                      "kind": "reference", "sample": f"unavailable: {e}"}
+        result["cpu_baseline"] = cpu_baseline_leg(result)
 
     if rank == 0:
         print(json.dumps(result), flush=True)
@@ -407,11 +480,37 @@ def main():
     return 0
 
 
-def run_reference_arm(args, cb):
+def cpu_baseline_leg(result):
+    """The unmodified reference invert_Qtm_her on one host core, a bounded
+    sample (runs of 1, 3 and 2 iterations on one column), extrapolated to
+    the iteration count that the same algorithm needed on the GPU."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bind as ob
+    if not ob.reference_available():
+        return {"value": None, "unit": "solves/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/libcvcref.so not built"}
+    its = result.get("fp64_plain_gpu", {}).get("iterations")
+    pool = ReferencePool(1)
+    try:
+        r = reference_rate(pool, 0, 1, n_conv=float(np.mean(its)) if its else None)
+    finally:
+        pool.close()
+    return {"value": r["value"], "unit": "solves/s", "cores": 1, "kind": "reference",
+            "sample": f"unmodified invert_Qtm_her (oracle/_ref, serial) on one 24^3x48 "
+                      f"point-source column: bounded runs of 1, 3 and 2 iterations, "
+                      f"{r['sec_per_iteration']:.2f} s per iteration, extrapolated to "
+                      f"{r['n_conv']:.1f} iterations per solve "
+                      + ("(the count the same algorithm needed on the GPU)" if its else
+                         "(measured to convergence)")}
+
+
+def run_reference_arm(args):
     """The reference's CPU solver on all usable host cores: one unmodified
-    invert_Qtm_her per worker process on its own column; each step is a
-    bounded sample (runs of one and two iterations per worker, whose
-    difference is the time of one iteration without the set-up)."""
+    invert_Qtm_her per worker process, each on its own column of the
+    workload.  Before the steps every worker solves its column to the
+    benchmark's residual, which measures the iteration count; each step is
+    then one bounded round (2 iterations per worker), and the rate is
+    workers / (seconds per iteration x iterations to convergence)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bind as ob
     if not ob.reference_available():
@@ -419,28 +518,37 @@ def run_reference_arm(args, cb):
                           "oracle/_ref/libcvcref.so not built (needs the reference tree at "
                           "build time)"}))
         return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     workers = ref_workers()
-    n_conv = 89.0  # iterations of invert_Qtm_her for these columns (FP64 mirror on the GPU)
-    times = []
-    for i in range(args.warmup + args.steps):
-        sec_it, _ = reference_iteration_seconds(workers, 1, 2)
-        if i >= args.warmup:
-            times.append(sec_it)
-    sec_it = float(np.mean(times))
-    value = workers / (sec_it * n_conv)
     cores = host_cores()
+    t_start = time.perf_counter()
+    pool = ReferencePool(workers)
+    try:
+        r = reference_rate(pool, args.warmup, args.steps,
+                           n_conv=float(args.ref_niter) if args.ref_niter else None)
+    finally:
+        pool.close()
+    value = r["value"]
+    ms_step = 1e3 * float(np.mean(r["step_wall_s"]))
+    how = ("measured: every worker solved its column to the benchmark's residual first"
+           if r["full"] else "given by --ref-niter")
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
-        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": sec_it * 2e3, "higher_is_better": True, "scaling": "weak",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "lattice": list(DIMS),
-                   "solver": "reference invert_Qtm_her (BiCGStab on Q^+Q), serial per process",
-                   "processes": workers},
+        "config": workload_config(world),
+        "run": {"solver": "reference invert_Qtm_her (BiCGStab on Q^+Q), serial per process",
+                "processes": workers, "iterations_to_convergence": r["n_conv"],
+                "iteration_count": how, "fixed_iterations_per_call": r["fixed_iterations"],
+                "sec_per_iteration": r["sec_per_iteration"], "full_solves": r["full"],
+                "total_s": time.perf_counter() - t_start},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "reference",
-                         "sample": f"{workers} processes x 1 + 2 invert_Qtm_her iterations per step "
-                                   f"({sec_it:.2f} s/iteration), extrapolated to {n_conv:.0f} "
-                                   f"iterations per solve; host has {cores} cores"},
+                         "sample": f"{workers} processes, each step one round of 2 "
+                                   f"invert_Qtm_her iterations per process "
+                                   f"({r['sec_per_iteration']:.2f} s per iteration), "
+                                   f"{r['n_conv']:.1f} iterations per solve ({how}); "
+                                   f"host has {cores} cores"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

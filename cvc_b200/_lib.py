@@ -18,7 +18,6 @@ CVCB_BREAKDOWN = -4
 CVCB_ERR_STATE = -5
 CVCB_ERR_NOMEM = -6
 CVCB_ERR_CUDA = -7
-CVCB_ERR_TIMEOUT = -8
 
 PREC_DOUBLE, PREC_SINGLE, PREC_HALF = 0, 1, 2
 

@@ -12,13 +12,17 @@
 // State: the globals below are the reference's own (declared here with the
 // types global.h gives them; the program that links this library defines
 // them).  One lattice context is created on first use on device
-// g_gpu_device_number and recreated when the extents change.  The gauge
-// field is uploaded when g_gauge_field points elsewhere or a sample of it
-// changed; call cvcb_compat_gauge_changed() after editing it in place.
+// g_gpu_device_number and recreated when the extents change.  Before every
+// call the whole gauge field is hashed on the host (one pass over 72*VOLUME
+// doubles, about 30 ms at 24^3x48), and it is uploaded again when
+// g_gauge_field points elsewhere or its contents changed, so a program that
+// edits the field in place never runs on stale links.
 //
 // Behaviour kept: argument meaning, field layouts, return values of the
-// solvers (iterations, -2, -3).  Fatal library errors print a message and
+// solvers (iterations, -2, -3; a broken-down BiCGStab, which the C ABI
+// reports as CVCB_BREAKDOWN, returns -3 here as in the reference).  Fatal library errors print a message and
 // exit(1), as the reference's EXIT() does.  The solvers print nothing.
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -44,7 +48,7 @@ namespace {
 cvcb_lattice *g_ctx = nullptr;
 int g_dims[4] = {0, 0, 0, 0};
 const double *g_gauge_ptr = nullptr;
-double g_gauge_sample[64];
+uint64_t g_gauge_hash = 0;
 bool g_force_upload = false;
 
 void fail(const char *where, int rc) {
@@ -52,9 +56,19 @@ void fail(const char *where, int rc) {
   std::exit(1);
 }
 
-void sample_gauge(double *out) {
+// Hash of the field's bits: four independent multiply-xor lanes over the
+// 64-bit words (word position enters through the lane and the order), so
+// any change of any bit of any link changes it with probability 1 - 2^-64.
+uint64_t hash_gauge() {
   const long n = 72L * cvc::VOLUME;
-  for (int k = 0; k < 64; ++k) out[k] = cvc::g_gauge_field[(long)k * (n / 64)];
+  const uint64_t *w = reinterpret_cast<const uint64_t *>(cvc::g_gauge_field);
+  const uint64_t m = 0x9E3779B97F4A7C15ull;
+  uint64_t h[4] = {1, 2, 3, 4};
+  long i = 0;
+  for (; i + 4 <= n; i += 4)
+    for (int k = 0; k < 4; ++k) h[k] = (h[k] ^ w[i + k]) * m + (h[k] >> 29);
+  for (; i < n; ++i) h[0] = (h[0] ^ w[i]) * m + (h[0] >> 29);
+  return (h[0] * 3 + h[1]) * 5 + (h[2] * 7 + h[3]) * 11;
 }
 
 cvcb_lattice *ctx() {
@@ -74,13 +88,12 @@ cvcb_lattice *ctx() {
     std::fprintf(stderr, "[cvc-b200] g_gauge_field is not allocated\n");
     std::exit(1);
   }
-  double s[64];
-  sample_gauge(s);
-  if (g_force_upload || g_gauge_ptr != g_gauge_field || std::memcmp(s, g_gauge_sample, sizeof s)) {
+  const uint64_t h = hash_gauge();
+  if (g_force_upload || g_gauge_ptr != g_gauge_field || h != g_gauge_hash) {
     rc = cvcb_upload_gauge(g_ctx, g_gauge_field);
     if (rc < 0) fail("cvcb_upload_gauge", rc);
     g_gauge_ptr = g_gauge_field;
-    std::memcpy(g_gauge_sample, s, sizeof s);
+    g_gauge_hash = h;
     g_force_upload = false;
   }
   return g_ctx;
@@ -92,6 +105,8 @@ void check(const char *where, int rc) {
 
 }  // namespace
 
+// Forces the next call to upload the gauge field (the hash already detects
+// every in-place change; kept for programs that call it).
 extern "C" void cvcb_compat_gauge_changed(void) { g_force_upload = true; }
 
 namespace cvc {
@@ -128,6 +143,7 @@ void spinor_scalar_product_re(double *r, double *xi, double *phi, int V) {
 int invert_Qtm(double *xi, double *phi, int kwork) {
   (void)kwork;
   const int rc = cvcb_invert_Qtm(ctx(), xi, phi, solver_precision, niter_max, nullptr);
+  if (rc == CVCB_BREAKDOWN) return CVCB_NO_CONVERGENCE;  // the reference's -3
   if (rc < 0 && rc != CVCB_ERR_NULL && rc != CVCB_NO_CONVERGENCE) fail("invert_Qtm", rc);
   return rc;
 }
@@ -135,6 +151,7 @@ int invert_Qtm(double *xi, double *phi, int kwork) {
 int invert_Qtm_her(double *xi, double *phi, int kwork) {
   (void)kwork;
   const int rc = cvcb_invert_Qtm_her(ctx(), xi, phi, solver_precision, niter_max, nullptr);
+  if (rc == CVCB_BREAKDOWN) return CVCB_NO_CONVERGENCE;  // the reference's -3
   if (rc < 0 && rc != CVCB_ERR_NULL && rc != CVCB_NO_CONVERGENCE) fail("invert_Qtm_her", rc);
   return rc;
 }

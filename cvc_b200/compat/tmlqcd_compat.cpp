@@ -13,7 +13,9 @@
 //   ThetaT, ThetaX, ThetaY, ThetaZ  boundary phases in units of pi/L
 //                                   (default 1, 0, 0, 0: antiperiodic in time,
 //                                   as CVC's BCangle)
-//   SolverPrecision                 squared relative residual (default 1e-20)
+//   SolverPrecision                 squared residual |b - D x|^2 (default 1e-20);
+//                                   absolute, as in tmLQCD, unless
+//   UseRelativePrecision            is yes: then relative to |b|^2 (default no)
 //   MaxSolverIterations             (default 20000)
 //   PropagatorFilePrefix            for write_prop (default "source")
 //   GPUDevice                       CUDA device (default 0)
@@ -41,6 +43,7 @@ namespace {
 struct Operator {
   double kappa = 0.125, two_kappa_mu = 0.0, precision = 1e-20;
   int max_iter = 20000;
+  bool relative = false;  // SolverPrecision relative to |b|^2 (tmLQCD: absolute)
 };
 
 struct State {
@@ -71,6 +74,7 @@ bool set_op_key(Operator &op, const std::string &k, const std::string &v) {
   else if (k == "2kappamu") op.two_kappa_mu = std::atof(v.c_str());
   else if (k == "solverprecision") op.precision = std::atof(v.c_str());
   else if (k == "maxsolveriterations") op.max_iter = std::atoi(v.c_str());
+  else if (k == "userelativeprecision") op.relative = lower(trim(v)) == "yes";
   else return false;
   return true;
 }
@@ -209,7 +213,16 @@ int tmLQCD_invert(double *const propagator, double *const source, const int op_i
   cvcb_solver_defaults(&p);
   p.precision = g.gpu_precision;
   p.link_recon = g.gpu_precision == CVCB_PREC_DOUBLE ? 18 : 12;
-  p.tol = std::sqrt(op.precision);
+  // the batched solver stops on |b - Q x| / |b|; tmLQCD's D x' = b with
+  // x' = x / (2 kappa) has the same residual b - Q x
+  double rel2 = op.precision;
+  if (!op.relative) {  // absolute: |b - Q x|^2 <= precision
+    const size_t nb = (size_t)24 * g.T * g.LX * g.LY * g.LZ;
+    double b2 = 0.0;
+    for (size_t i = 0; i < nb; ++i) b2 += source[i] * source[i];
+    if (b2 > 0) rel2 = op.precision / b2;
+  }
+  p.tol = std::sqrt(rel2);
   p.max_iter = op.max_iter;
   cvcb_solver_stats st;
   double *x[1] = {propagator};

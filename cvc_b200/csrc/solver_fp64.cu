@@ -289,8 +289,13 @@ int invert_bicgstab(cvcb_lattice *L, bool her, double *xi, const double *phi, do
   CVCB_TRY(spinor_out(L, xi, x, g.V));
   if (!converged) {
     CVCB_CUDA(cudaStreamSynchronize(L->stream));
-    set_error("no convergence after %d iterations (relative residual^2 %g)%s", niter,
-              hs.norm / hs.normb, hs.done == 2 ? ", recursion broke down" : "");
+    if (hs.done == 2) {  // a non-finite alpha, omega or beta stopped the recursion
+      set_error("BiCGStab broke down after %d iterations (relative residual^2 %g)", hs.niter,
+                hs.norm / hs.normb);
+      return CVCB_BREAKDOWN;
+    }
+    set_error("no convergence after %d iterations (relative residual^2 %g)", niter,
+              hs.norm / hs.normb);
     return CVCB_NO_CONVERGENCE;
   }
   if (true_res2) {

@@ -1000,10 +1000,27 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   // iterations each rhs is predicted to need (from its measured convergence
   // rate) so that the last chunk does not overshoot convergence.
   const int kmax = 10;
-  cudaGraphExec_t gexec = nullptr;
+  // The executable graph and the stencil timing events are released on every
+  // exit path, early error returns included.
+  struct Release {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<typename Batch<SF, XF, LF>::Rec> *recs = nullptr;
+    ~Release() {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (recs) {
+        for (auto &r : *recs) {
+          cudaEventDestroy(r.a);
+          cudaEventDestroy(r.b);
+        }
+        recs->clear();
+      }
+    }
+  } release;
+  release.recs = &B.recs;
+  cudaGraphExec_t &gexec = release.exec;
   long long graph_nodes = 0;
   if (P->use_graph) {
-    cudaGraph_t graph;
+    cudaGraph_t graph = nullptr;
     const long long before = L->nlaunch;
     CVCB_CUDA(cudaStreamBeginCapture(L->stream, cudaStreamCaptureModeThreadLocal));
     B.capturing = true;
@@ -1012,10 +1029,14 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     B.prof_rec = false;
     B.capturing = false;
     cudaError_t ec = cudaStreamEndCapture(L->stream, &graph);
-    if (rc != CVCB_OK) return rc;
-    CVCB_CUDA(ec);
-    CVCB_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
+    if (rc != CVCB_OK || ec != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (rc != CVCB_OK) return rc;
+      CVCB_CUDA(ec);
+    }
+    ec = cudaGraphInstantiate(&gexec, graph, 0);
     cudaGraphDestroy(graph);
+    CVCB_CUDA(ec);
     graph_nodes = L->nlaunch - before;  // kernels per graph launch
     L->nlaunch = before;
   }
@@ -1147,6 +1168,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     CVCB_TRY(put_flags(L, B.S.done, done, n));
   }
   if (gexec) cudaGraphExecDestroy(gexec);
+  gexec = nullptr;
   for (auto &r : B.recs) {
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);

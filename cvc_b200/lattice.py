@@ -171,10 +171,13 @@ class Lattice:
 
     # -- solvers (invert_Qtm.c) ------------------------------------------
     def invert_Qtm(self, xi, phi, solver_precision, niter_max, return_residual=False):
-        """BiCGStab on Q.  Returns niter, -2 or -3 as the reference does."""
+        """BiCGStab on Q.  Returns niter, -2 or -3 as the reference does (-3
+        also for a broken-down recursion, which the C ABI reports as -4)."""
         tr = np.zeros(1)
         rc = self._lib.cvcb_invert_Qtm(self._h, ptr(xi), ptr(phi), float(solver_precision),
                                        int(niter_max), ptr(tr))
+        if rc == _lib.CVCB_BREAKDOWN:  # the reference returns -3 here
+            rc = _lib.CVCB_NO_CONVERGENCE
         if rc < 0 and rc not in (_lib.CVCB_ERR_NULL, _lib.CVCB_NO_CONVERGENCE):
             raise CvcbError("invert_Qtm", rc)
         return (rc, float(tr[0])) if return_residual else rc
@@ -184,6 +187,8 @@ class Lattice:
         tr = np.zeros(1)
         rc = self._lib.cvcb_invert_Qtm_her(self._h, ptr(xi), ptr(phi), float(solver_precision),
                                            int(niter_max), ptr(tr))
+        if rc == _lib.CVCB_BREAKDOWN:  # the reference returns -3 here
+            rc = _lib.CVCB_NO_CONVERGENCE
         if rc < 0 and rc not in (_lib.CVCB_ERR_NULL, _lib.CVCB_NO_CONVERGENCE):
             raise CvcbError("invert_Qtm_her", rc)
         return (rc, float(tr[0])) if return_residual else rc

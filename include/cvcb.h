@@ -32,7 +32,10 @@ extern "C" {
 #endif
 
 /* Status codes.  -2 and -3 are the reference's own solver returns
- * (invert_Qtm.c:112-113, 242-251); the others are new. */
+ * (invert_Qtm.c:112-113, 242-251); the others are new.  CVCB_BREAKDOWN:
+ * a BiCGStab recursion scalar (alpha, omega, beta) became non-finite, which
+ * the reference reports as -3 (invert_Qtm.c:213-216, 250); the namespace-cvc
+ * drop-in and the Python mirror map it back to -3. */
 #define CVCB_OK 0
 #define CVCB_ERR_ARG (-1)
 #define CVCB_ERR_NULL (-2)
@@ -41,7 +44,6 @@ extern "C" {
 #define CVCB_ERR_STATE (-5)
 #define CVCB_ERR_NOMEM (-6)
 #define CVCB_ERR_CUDA (-7)
-#define CVCB_ERR_TIMEOUT (-8)
 
 typedef struct cvcb_lattice cvcb_lattice;
 
@@ -179,7 +181,8 @@ int cvcb_spinor_scalar_product_re(cvcb_lattice *lat, double *r, const double *xi
  * |r|^2 <= solver_precision * |phi|^2 (squared norms, invert_Qtm.c:201).
  * xi holds the start guess on entry and the solution on exit.
  * Returns the iteration count, CVCB_ERR_NULL or CVCB_NO_CONVERGENCE as the
- * reference does.  true_res2 (may be NULL) receives |Q xi - phi|^2/|phi|^2.
+ * reference does, or CVCB_BREAKDOWN where the reference returns -3 after
+ * its recursion produced a non-finite scalar.  true_res2 (may be NULL) receives |Q xi - phi|^2/|phi|^2.
  * ------------------------------------------------------------------- */
 
 /* BiCGStab on Q.  Replaces int invert_Qtm(double *xi, double *phi,

@@ -6,7 +6,10 @@
  *
  *  - one process, one GPU: the MPI parameters describe a single rank;
  *  - operators: each "BeginOperator ... EndOperator" block of the input file
- *    (kappa, 2KappaMu, SolverPrecision, MaxSolverIterations) is one op_id;
+ *    (kappa, 2KappaMu, SolverPrecision, MaxSolverIterations,
+ *    UseRelativePrecision) is one op_id; SolverPrecision is the squared
+ *    residual |b - D x|^2, absolute unless UseRelativePrecision = yes, as in
+ *    tmLQCD's input files;
  *  - tmLQCD_invert returns the solution of D psi = source with tmLQCD's
  *    normalisation D = 2 kappa Q = (1 + 2 i kappa mu g5) - kappa H, i.e.
  *    psi = Q^-1 source / (2 kappa), in CVC's field layout;

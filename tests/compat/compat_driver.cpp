@@ -6,13 +6,16 @@
 // programs do, reads a raw gauge field and spinor, and calls the reference
 // interface: Q_phi_tbc, Qf5, the scalar products, invert_Qtm_her, and the
 // reference's own check_source (cvc_utils.c), which itself calls Q_phi and
-// spinor_scalar_product_re -- now bound to the GPU versions.
+// spinor_scalar_product_re -- now bound to the GPU versions.  Then the
+// point-source breakdown of invert_Qtm, and Q_phi_tbc after one link of
+// g_gauge_field was edited in place.
 //
 // usage: compat_driver T LX LY LZ kappa mu gauge.bin phi.bin out_prefix
 #define MAIN_PROGRAM
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <math.h>
 #include "global.h"
 #include "cvc_complex.h"
 #include "cvc_geometry.h"
@@ -72,5 +75,22 @@ int main(int argc, char **argv) {
   printf("niter %d\n", n);
   write_raw(argv[9], "x", xi, (size_t)24 * VOLUME);
   check_source(xi, work, g_mu, 0, 4);
+
+  // plain BiCGStab breaks down on a point source: the reference's -3
+  memset(xi, 0, sizeof(double) * 24 * VOLUME);
+  printf("breakdown %d\n", invert_Qtm(xi, phi, 0));
+
+  // edit one link in place (site 37, mu 2, times e^{0.7 i}) and apply the
+  // operator again: the library must notice and upload the field again
+  read_raw(argv[8], phi, (size_t)24 * VOLUME);
+  double *u = g_gauge_field + 18 * (4 * 37 + 2);
+  const double c = cos(0.7), s = sin(0.7);
+  for (int k = 0; k < 9; ++k) {
+    const double re = u[2 * k], im = u[2 * k + 1];
+    u[2 * k] = c * re - s * im;
+    u[2 * k + 1] = s * re + c * im;
+  }
+  Q_phi_tbc(xi, phi);
+  write_raw(argv[9], "Q_phi_tbc_edit", xi, (size_t)24 * VOLUME);
   return 0;
 }

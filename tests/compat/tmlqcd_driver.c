@@ -2,7 +2,8 @@
  * parameters, :206-216 gauge field, :436-547 the two operators x 12
  * spin-colour point-source inversions at the unshifted source, :1032
  * finalise) against libcvcb200_tmlqcd.so, and dumps the gauge field it got
- * and the propagators as raw doubles for the test to compare.
+ * and the propagators as raw doubles for the test to compare; then one
+ * inversion of a source of norm 1e-3 (absolute SolverPrecision).
  *   tmlqcd_driver -f <input> <t> <x> <y> <z> <outdir> */
 #include <stdio.h>
 #include <stdlib.h>
@@ -46,6 +47,11 @@ int main(int argc, char **argv) {
       snprintf(name, sizeof name, "prop.%u.%02d.raw", op, ia);
       if (dump(out, name, prop, 24 * V)) return 103;
     }
+  /* a source of norm 1e-3: SolverPrecision is absolute, as in tmLQCD */
+  memset(source, 0, 24 * V * sizeof(double));
+  source[24 * ix] = 1e-3;
+  if (tmLQCD_invert(prop, source, 0, 0) != 0) exit(8);
+  if (dump(out, "prop.scaled.raw", prop, 24 * V)) return 104;
   free(source);
   free(prop);
   tmLQCD_finalise();

@@ -23,7 +23,8 @@ REF_DIR = os.path.join(ORACLE_DIR, "_ref")
 REF_LIB = os.path.join(REF_DIR, "libcvcref.so")
 REF_OMP_LIB = os.path.join(REF_DIR, "libcvcref_omp.so")
 REF_CONTRACT = os.path.join(REF_DIR, "cvc_exact2_xspace")
-REFERENCE_TREE = "/root/reference"
+# where the reference sources lie (only read at build time, to compile them)
+REFERENCE_TREE = os.environ.get("CVC_REFERENCE_TREE", "/root/reference")
 
 _P = ctypes.c_void_p
 _D = ctypes.c_double
@@ -47,6 +48,16 @@ def build_oracle():
 
 def reference_available():
     return os.path.exists(REF_LIB)
+
+
+def reference_ranlxd(n, seed, level=1):
+    """The first n numbers of the reference's ranlxd stream (ranlxd.c) after
+    rlxd_init(level, seed), without initialising a lattice."""
+    lib = Reference._lib if Reference._lib is not None else ctypes.CDLL(REF_LIB)
+    r = np.zeros(n)
+    lib.ref_rlxd_init(level, seed)
+    lib.ref_ranlxd(_p(r), n)
+    return r
 
 
 class OrcLattice(ctypes.Structure):

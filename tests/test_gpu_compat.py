@@ -38,6 +38,7 @@ def test_reference_program_links_and_runs_on_gpu(cb, oracle_mod):
         q = np.fromfile(os.path.join(d, "out.Q_phi_tbc"))
         f5 = np.fromfile(os.path.join(d, "out.Qf5_minus"))
         x = np.fromfile(os.path.join(d, "out.x"))
+        q_edit = np.fromfile(os.path.join(d, "out.Q_phi_tbc_edit"))
     assert rel_err(q, orc.Q_phi_tbc(phi)) < 1e-14
     qf5 = orc.Qf5(phi, -mu)
     assert rel_err(f5, qf5) < 1e-14
@@ -54,3 +55,14 @@ def test_reference_program_links_and_runs_on_gpu(cb, oracle_mod):
     # the reference's check_source printed |Q x - delta|^2 via the GPU Q_phi
     res = [l for l in lines if "norm of A x - delta" in l][0]
     assert float(res.split("=")[1]) < 1e-18
+    # the point-source breakdown keeps the reference's return value
+    assert int([l for l in lines if l.startswith("breakdown")][0].split()[1]) == -3
+    # one link edited in place (site 37, mu 2, times e^{0.7 i}) is picked up
+    ge = g.copy()
+    u = ge[18 * (4 * 37 + 2):18 * (4 * 37 + 2) + 18].view(np.complex128)
+    u *= np.exp(0.7j)
+    orc.set_gauge(ge)
+    want = orc.Q_phi_tbc(phi)
+    assert rel_err(q_edit, want) < 1e-14
+    orc.set_gauge(g)
+    assert rel_err(q_edit, orc.Q_phi_tbc(phi)) > 1e-6

@@ -57,6 +57,13 @@ def test_invert_Qtm_breaks_down_on_point_source(env):
     assert lat.invert_Qtm(x, b, 1e-20, 50) == -3
     rc, _, _ = orc.invert(b, 1e-20, 50, her=False)
     assert rc == -3
+    # the C ABI names the cause: CVCB_BREAKDOWN, not plain non-convergence
+    from cvc_b200 import _lib
+    from cvc_b200.lattice import ptr
+    x[:] = 0
+    rc = lat._lib.cvcb_invert_Qtm(lat._h, ptr(x), ptr(b), 1e-20, 50, None)
+    assert rc == _lib.CVCB_BREAKDOWN
+    assert "broke down" in lat._lib.cvcb_last_error().decode()
 
 
 def test_invert_Qtm_random_source_subcritical(cb, oracle_mod):

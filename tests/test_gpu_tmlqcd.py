@@ -4,7 +4,8 @@ file with two operators (+2 kappa mu and -2 kappa mu), an ILDG gauge file
 written by cvc_b200.lime, 2 x 12 point-source inversions.  Propagators must
 equal the oracle's FP64 solutions of Q x = b divided by 2 kappa (tmLQCD's
 normalisation) to 1e-8, the gauge field pointer must hold the file's field,
-and the propagator written with write_prop must read back."""
+the propagator written with write_prop must read back, and SolverPrecision
+is an absolute squared residual as in tmLQCD."""
 import os
 import shutil
 import subprocess
@@ -57,5 +58,15 @@ def test_tmlqcd_abi(cb, oracle_mod, tmp_path):
             _, x, _ = orc.invert(b, 1e-26, 5000, her=True)
             p = np.fromfile(tmp_path / f"prop.{op}.{ia:02d}.raw")
             assert rel_err(p, x / (2 * KAPPA)) < 1e-8, (op, ia)
+    # SolverPrecision 1e-24 is absolute: for a source of norm 1e-3 the solve
+    # reaches |b - Q x|^2 <= 1e-24, i.e. a relative 1e-9 (not 1e-12)
+    orc.set_params(KAPPA, mu)
+    b = np.zeros(24 * V)
+    b[24 * ix] = 1e-3
+    p = np.fromfile(tmp_path / "prop.scaled.raw")
+    r = b - orc.Q_phi_tbc(2 * KAPPA * p)
+    assert np.dot(r, r) <= 1e-24
+    _, x, _ = orc.invert(b, 1e-26, 5000, her=True)
+    assert rel_err(p, x / (2 * KAPPA)) < 1e-5
     written, _ = lime.read_lime_spinor(tmp_path / "source.0005.00.inverted", DIMS, 0)
     assert np.array_equal(written, np.fromfile(tmp_path / "prop.0.00.raw"))

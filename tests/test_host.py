@@ -189,3 +189,16 @@ def test_tmlqcd_wrapper_before_and_without_init(cb, tmp_path):
     assert init(open_block) == 1
     assert lib.tmLQCD_read_gauge(0) == 1     # still not initialised
     assert lib.tmLQCD_finalise() == 0
+
+
+def test_gauge_recipe_restatement(cb):
+    """The numpy restatement of the gauge recipe (used where the CUDA library
+    must not be loaded: the reference arm of bench.py) agrees with the
+    library's generator to rounding."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gauge_recipe
+    for dims, eps, seed in [((8, 4, 4, 4), 0.3, 1234), ((4, 6, 2, 4), 0.25, 11)]:
+        a = cb.gauge_random(*dims, eps, seed)
+        b = gauge_recipe.gauge_random(*dims, eps, seed, cb.ranlxd)
+        assert np.max(np.abs(a - b)) < 1e-14

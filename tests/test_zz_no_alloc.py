@@ -66,3 +66,34 @@ def test_noalloc_partial_volume_and_limits(cb):
     h = np.zeros(2)
     assert lib.cvcb_spinor_scalar_product_co_noalloc(0, h.ctypes.data, da.data_ptr(),
                                                      db.data_ptr(), V, None) == -1
+
+
+def test_noalloc_allocates_nothing_on_a_caller_stream(cb):
+    """The property the entry point exists for: after a first call on the
+    device (which looks up the fixed array's address), further calls change
+    no device memory usage, also when enqueued on a stream of the caller's
+    (stream-ordered: the result is ready when that stream reaches it)."""
+    torch = pytest.importorskip("torch")
+    lib = cb.load()
+    V = 4096
+    a = seeded(11, 24 * V)
+    b = seeded(12, 24 * V)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    w = torch.zeros(2, dtype=torch.float64, device="cuda")
+    assert lib.cvcb_spinor_scalar_product_co_noalloc(0, w.data_ptr(), da.data_ptr(),
+                                                     db.data_ptr(), V, None) == 0
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    free0, _ = torch.cuda.mem_get_info()
+    x = (a[0::2] + 1j * a[1::2])
+    y = (b[0::2] + 1j * b[1::2])
+    ref = np.sum(np.conj(x) * y)
+    for _ in range(3):
+        w.zero_()
+        torch.cuda.synchronize()
+        assert lib.cvcb_spinor_scalar_product_co_noalloc(0, w.data_ptr(), da.data_ptr(),
+                                                         db.data_ptr(), V, s.cuda_stream) == 0
+        s.synchronize()
+        assert abs(complex(w[0].item(), w[1].item()) - ref) <= 1e-13 * abs(ref)
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
