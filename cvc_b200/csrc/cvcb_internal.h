@@ -195,6 +195,10 @@ struct cvcb_lattice {
   float4 *U32c = nullptr;   // [4][3][V], raw rows 0,1
   float2 *U32f = nullptr;   // [4][9][V], phased (18-real single)
   uint2 *U16c = nullptr;    // [4][3][V], raw rows 0,1 in half
+  // the same single-precision forms tiled by 32 even/odd link indices (for
+  // the pair-tiled stencil): [V/32][4][9][32] and [V/32][4][3][32]
+  float2 *UT32f = nullptr;
+  float4 *UT32c = nullptr;
 
   // reduction scratch: per-block partials, a completion counter, results
   double *partials = nullptr;  // [kMaxRedBlocks * 4]

@@ -268,6 +268,11 @@ struct HopArgs {
   // warp in the row; null = off
   double *dot_part;
   int dot_np;
+  // optional (k_eo_hop_pt with the residual update): instead of storing
+  // out, r -= alpha[rhs] * out on the field set `rup` (and dot_part gets
+  // |r|^2)
+  SF rup;
+  const double *alpha;
 };
 
 // |a|^2 of one site, accumulated in FP64

@@ -140,7 +140,8 @@ __device__ inline double2 cmul(double2 a, double2 b) {
 
 __global__ void k_gauge_forms(const double2 *__restrict__ raw, Geom g, double4 ph01, double4 ph23,
                               double2 *__restrict__ U64, float4 *__restrict__ U32c,
-                              float2 *__restrict__ U32f, uint2 *__restrict__ U16c) {
+                              float2 *__restrict__ U32f, uint2 *__restrict__ U16c,
+                              float2 *__restrict__ UT32f, float4 *__restrict__ UT32c) {
   const int lex = blockIdx.x * blockDim.x + threadIdx.x;
   if (lex >= g.V) return;
   const int eo = lex_to_eo(g, lex);
@@ -157,12 +158,17 @@ __global__ void k_gauge_forms(const double2 *__restrict__ raw, Geom g, double4 p
       w[k] = cmul(u[k], ph[mu]);
       U64[((size_t)mu * 9 + k) * g.V + eo] = w[k];
       U32f[((size_t)mu * 9 + k) * g.V + eo] = make_float2((float)w[k].x, (float)w[k].y);
+      // tiled by 32 even/odd indices: [eo / 32][mu][k][eo % 32]
+      UT32f[(((size_t)(eo >> 5) * 4 + mu) * 9 + k) * 32 + (eo & 31)] =
+          make_float2((float)w[k].x, (float)w[k].y);
     }
     // 12-real forms: rows 0 and 1 of the phased link
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const double2 a = w[2 * q], b = w[2 * q + 1];
       U32c[((size_t)mu * 3 + q) * g.V + eo] =
+          make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+      UT32c[(((size_t)(eo >> 5) * 4 + mu) * 3 + q) * 32 + (eo & 31)] =
           make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
       __half2 h0 = __floats2half2_rn((float)a.x, (float)a.y);
       __half2 h1 = __floats2half2_rn((float)b.x, (float)b.y);
@@ -182,6 +188,9 @@ static int build_gauge_forms(cvcb_lattice *L) {
     CVCB_CUDA(cudaMalloc(&L->U32c, V * 12 * sizeof(float4)));
     CVCB_CUDA(cudaMalloc(&L->U32f, V * 36 * sizeof(float2)));
     CVCB_CUDA(cudaMalloc(&L->U16c, V * 12 * sizeof(uint2)));
+    const size_t tiles = (V + 31) / 32;
+    CVCB_CUDA(cudaMalloc(&L->UT32f, tiles * 32 * 36 * sizeof(float2)));
+    CVCB_CUDA(cudaMalloc(&L->UT32c, tiles * 32 * 12 * sizeof(float4)));
   }
   void *raw;
   CVCB_TRY(ensure_buffer(L, SLOT_STAGE_A, V * 72 * sizeof(double), &raw));
@@ -190,7 +199,8 @@ static int build_gauge_forms(cvcb_lattice *L) {
   const double *ph = L->phase;
   k_gauge_forms<<<(g.V + 127) / 128, 128, 0, L->stream>>>(
       static_cast<const double2 *>(raw), g, make_double4(ph[0], ph[1], ph[2], ph[3]),
-      make_double4(ph[4], ph[5], ph[6], ph[7]), L->U64, L->U32c, L->U32f, L->U16c);
+      make_double4(ph[4], ph[5], ph[6], ph[7]), L->U64, L->U32c, L->U32f, L->U16c, L->UT32f,
+      L->UT32c);
   CVCB_LAUNCHED(L);
   CVCB_CUDA(cudaStreamSynchronize(L->stream));
   return CVCB_OK;
@@ -299,6 +309,8 @@ int cvcb_lattice_destroy(cvcb_lattice *L) {
   cudaFree(L->U32c);
   cudaFree(L->U32f);
   cudaFree(L->U16c);
+  cudaFree(L->UT32f);
+  cudaFree(L->UT32c);
   cudaFree(L->partials);
   cudaFree(L->red_counter);
   cudaFree(L->red_result);

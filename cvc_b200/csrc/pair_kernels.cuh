@@ -1,0 +1,362 @@
+// Pair-tiled storage and its kernels for the FP32 inner iterations of the
+// batched solver.
+//
+// Right-hand sides 2q and 2q+1 ("pair q") are stored interleaved per complex
+// spin-colour component, so that one 16-byte load yields both right-hand
+// sides of a component in the register order of the packed FP32x2
+// instructions (FFMA2/FADD2/FMUL2):
+//   float4 P[pair][tile = j / 32][component k = 0..11][j % 32]
+//   float4 = (re of rhs 2q, re of rhs 2q+1, im of rhs 2q, im of rhs 2q+1)
+// A warp reading component k of 32 consecutive sites reads 512 contiguous
+// bytes; the 12 components of one site lie at fixed offsets (k * 512 B) from
+// one address, so a neighbour costs one address computation, not twelve.
+// Links are tiled the same way (tile = even/odd link index / 32), with 18
+// reals (phase multiplied in; nothing to rebuild) or 12 reals (rows 0, 1;
+// row 2 rebuilt in registers).
+//
+// Compared with per-rhs structure-of-arrays storage packed into FP32x2 pairs
+// after the loads (k_eo_hop_x2), the stencil needs no register moves to form
+// the pairs, projects and reconstructs both right-hand sides with packed
+// additions, and applies the site-diagonal epilogue in packed arithmetic.
+#pragma once
+
+#include "eo_kernels.cuh"
+#include "reduce.cuh"
+
+namespace cvcb {
+
+constexpr int kTile = 32;
+
+__device__ __forceinline__ CP cp_of(float4 v) {
+  CP c;
+  c.re = make_float2(v.x, v.y);
+  c.im = make_float2(v.z, v.w);
+  return c;
+}
+__device__ __forceinline__ float4 f4_of(const CP &c) {
+  return make_float4(c.re.x, c.re.y, c.im.x, c.im.y);
+}
+
+// FP32 pair-tiled field set: pair pr, half-lattice site j.
+struct P32 {
+  using R = float;
+  float4 *p;
+  size_t pstride;  // float4 per pair (tiles x 12 x 32)
+  __device__ __forceinline__ float4 *at(int pr, int j) const {
+    return p + (size_t)pr * pstride + (size_t)(j >> 5) * (12 * kTile) + (j & (kTile - 1));
+  }
+  __device__ __forceinline__ SpinorPair load_pair(int pr, int j) const {
+    const float4 *q = at(pr, j);
+    SpinorPair s;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) s.c[k / 3][k % 3] = cp_of(__ldg(q + k * kTile));
+    return s;
+  }
+  __device__ __forceinline__ void store_pair(int pr, int j, const SpinorPair &s) const {
+    float4 *q = at(pr, j);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) q[k * kTile] = f4_of(s.c[k / 3][k % 3]);
+  }
+  // one lane of a pair (lane 0: rhs 2 pr, lane 1: rhs 2 pr + 1); the other
+  // lane's values are left as they are
+  __device__ __forceinline__ void store_lane(int pr, int lane, int j, const SpinorPair &s) const {
+    float *q = reinterpret_cast<float *>(at(pr, j)) + lane;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      const CP &c = s.c[k / 3][k % 3];
+      q[4 * kTile * k] = lane ? c.re.y : c.re.x;
+      q[4 * kTile * k + 2] = lane ? c.im.y : c.im.x;
+    }
+  }
+  // per-rhs access (for the kernels that run once per reliable update)
+  __device__ __forceinline__ Spinor<float> load(int r, int j) const {
+    const float4 *q = at(r >> 1, j);
+    const bool b = r & 1;
+    Spinor<float> s;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      const float4 v = __ldg(q + k * kTile);
+      s.c[k / 3][k % 3] = cx(b ? v.y : v.x, b ? v.w : v.z);
+    }
+    return s;
+  }
+  __device__ __forceinline__ Spinor<float> load_raw(int r, int j, float &nm) const {
+    nm = 1.f;
+    return load(r, j);
+  }
+  __device__ __forceinline__ void store(int r, int j, const Spinor<float> &s) const {
+    float *q = reinterpret_cast<float *>(at(r >> 1, j)) + (r & 1);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      q[4 * kTile * k] = s.c[k / 3][k % 3].re;
+      q[4 * kTile * k + 2] = s.c[k / 3][k % 3].im;
+    }
+  }
+};
+
+inline size_t p32_pair_float4(int Vh) { return (size_t)((Vh + kTile - 1) / kTile) * 12 * kTile; }
+
+// 18-real phased links, tiled: float2 U[idx / 32][mu][9][idx % 32]
+struct LT32f {
+  using R = float;
+  static constexpr bool kPhased = true;
+  const float2 *U;
+  float2 ph[4];  // unused: the phase is multiplied in
+  __device__ __forceinline__ Link<float> load(int mu, int idx) const {
+    const float2 *q = U + (size_t)(idx >> 5) * (36 * kTile) + mu * 9 * kTile + (idx & (kTile - 1));
+    Link<float> L;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float2 v = __ldg(q + k * kTile);
+      L.m[k / 3][k % 3] = cx(v.x, v.y);
+    }
+    return L;
+  }
+};
+
+// 12-real phased links (rows 0, 1), tiled: float4 U[idx / 32][mu][3][idx % 32];
+// row 2 = e^{3 i theta_mu} conj(row0 x row1) (ph = e^{3 i theta_mu})
+struct LT32c {
+  using R = float;
+  static constexpr bool kPhased = true;
+  const float4 *U;
+  float2 ph[4];
+  __device__ __forceinline__ Link<float> load(int mu, int idx) const {
+    const float4 *q = U + (size_t)(idx >> 5) * (12 * kTile) + mu * 3 * kTile + (idx & (kTile - 1));
+    Link<float> L;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 v = __ldg(q + k * kTile);
+      L.m[(2 * k) / 3][(2 * k) % 3] = cx(v.x, v.y);
+      L.m[(2 * k + 1) / 3][(2 * k + 1) % 3] = cx(v.z, v.w);
+    }
+    reconstruct_row2(L);
+    apply_row2_phase(L, ph[mu]);
+    return L;
+  }
+};
+
+inline size_t lt_tiles(int V) { return (size_t)(V + kTile - 1) / kTile; }
+
+// h = (1 + s g_mu) f projected to spins 0, 1, both rhs (table in
+// spinor_ops.cuh); with g5 on the input the sign of the lower spins flips
+template <int MU, int S>
+__device__ __forceinline__ HalfPair project_pair(const SpinorPair &f) {
+  HalfPair h;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const CP &f0 = f.c[0][c], &f1 = f.c[1][c], &f2 = f.c[2][c], &f3 = f.c[3][c];
+    if (MU == 0) {  // h0 = f0 - s f2, h1 = f1 - s f3
+      h.c[0][c].re = S > 0 ? sub2(f0.re, f2.re) : add2(f0.re, f2.re);
+      h.c[0][c].im = S > 0 ? sub2(f0.im, f2.im) : add2(f0.im, f2.im);
+      h.c[1][c].re = S > 0 ? sub2(f1.re, f3.re) : add2(f1.re, f3.re);
+      h.c[1][c].im = S > 0 ? sub2(f1.im, f3.im) : add2(f1.im, f3.im);
+    } else if (MU == 1) {  // h0 = f0 - s i f3, h1 = f1 - s i f2; i z = (-z.im, z.re)
+      h.c[0][c].re = S > 0 ? add2(f0.re, f3.im) : sub2(f0.re, f3.im);
+      h.c[0][c].im = S > 0 ? sub2(f0.im, f3.re) : add2(f0.im, f3.re);
+      h.c[1][c].re = S > 0 ? add2(f1.re, f2.im) : sub2(f1.re, f2.im);
+      h.c[1][c].im = S > 0 ? sub2(f1.im, f2.re) : add2(f1.im, f2.re);
+    } else if (MU == 2) {  // h0 = f0 - s f3, h1 = f1 + s f2
+      h.c[0][c].re = S > 0 ? sub2(f0.re, f3.re) : add2(f0.re, f3.re);
+      h.c[0][c].im = S > 0 ? sub2(f0.im, f3.im) : add2(f0.im, f3.im);
+      h.c[1][c].re = S > 0 ? add2(f1.re, f2.re) : sub2(f1.re, f2.re);
+      h.c[1][c].im = S > 0 ? add2(f1.im, f2.im) : sub2(f1.im, f2.im);
+    } else {  // h0 = f0 - s i f2, h1 = f1 + s i f3
+      h.c[0][c].re = S > 0 ? add2(f0.re, f2.im) : sub2(f0.re, f2.im);
+      h.c[0][c].im = S > 0 ? sub2(f0.im, f2.re) : add2(f0.im, f2.re);
+      h.c[1][c].re = S > 0 ? sub2(f1.re, f3.im) : add2(f1.re, f3.im);
+      h.c[1][c].im = S > 0 ? add2(f1.im, f3.re) : sub2(f1.im, f3.re);
+    }
+  }
+  return h;
+}
+
+// out = (a_s + i b_s) v per spin s (site-diagonal, per-spin coefficients)
+__device__ __forceinline__ void diag_pair(SpinorPair &o, const SpinorPair &v, const float (&a)[4],
+                                          const float (&b)[4], bool accumulate) {
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const CP &x = v.c[s][c];
+      float2 re = accumulate ? __ffma2_rn(bc(a[s]), x.re, o.c[s][c].re) : __fmul2_rn(bc(a[s]), x.re);
+      float2 im = accumulate ? __ffma2_rn(bc(a[s]), x.im, o.c[s][c].im) : __fmul2_rn(bc(a[s]), x.im);
+      re = __ffma2_rn(bc(-b[s]), x.im, re);
+      im = __ffma2_rn(bc(b[s]), x.re, im);
+      o.c[s][c].re = re;
+      o.c[s][c].im = im;
+    }
+}
+
+__device__ __forceinline__ float2 norm2_pair(const SpinorPair &v) {
+  float2 n = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      n = __ffma2_rn(v.c[s][c].re, v.c[s][c].re, n);
+      n = __ffma2_rn(v.c[s][c].im, v.c[s][c].im, n);
+    }
+  return n;
+}
+
+__device__ __forceinline__ void store_active(const P32 &f, int pr, int j, const SpinorPair &v,
+                                             bool act_a, bool act_b) {
+  if (act_a && act_b)
+    f.store_pair(pr, j, v);
+  else
+    f.store_lane(pr, act_a ? 0 : 1, j, v);
+}
+
+template <int MU, class LF>
+__device__ __forceinline__ void hop_pair_dir(SpinorPair &acc, const HopArgs<P32, LF> &A,
+                                             const SiteCoord &cd, int pr, int self, int qoff,
+                                             bool g5in) {
+  const Geom &g = A.eg.g;
+  {  // backward: (1 + g_mu) U_mu(x-mu)^+ in(x-mu)
+    const int j = nb_lex(g, cd, MU, -1) >> 1;
+    const Link<float> W = A.links.load(MU, qoff + j);
+    const SpinorPair f = A.in.load_pair(pr, j);
+    const HalfPair h = g5in ? project_pair<MU, -1>(f) : project_pair<MU, +1>(f);
+    accum_recon_pair(MU, +1, acc, link_mul_pair<true>(W, h));
+  }
+  {  // forward: (1 - g_mu) U_mu(x) in(x+mu)
+    const int j = nb_lex(g, cd, MU, +1) >> 1;
+    const Link<float> W = A.links.load(MU, self);
+    const SpinorPair f = A.in.load_pair(pr, j);
+    const HalfPair h = g5in ? project_pair<MU, +1>(f) : project_pair<MU, -1>(f);
+    accum_recon_pair(MU, -1, acc, link_mul_pair<false>(W, h));
+  }
+}
+
+// The even/odd stencil sweep (same operator as k_eo_hop) on pair-tiled
+// fields: thread = (site, rhs pair).  Directions in the order z, y, x, t (the
+// z and y neighbours of a block's sites are in L1 after z-).  A pair with one
+// inactive right-hand side computes both and stores only the active one;
+// with dot_part, per-warp partials of |out|^2 per rhs (as k_eo_hop_x2).
+// RUPD: the sweep that produces A p of a CG iteration updates the residual
+// instead, r -= alpha A p, and its partials are those of |r|^2; A p itself
+// is not stored (CG needs it for nothing else).
+template <class LF, bool G5IN, bool G5HOP, bool AUX, bool RUPD = false>
+__global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_pt(HopArgs<P32, LF> A) {
+  const int pr = blockIdx.x * blockDim.y + threadIdx.y;
+  const int ra = 2 * pr;
+  if (ra >= A.nrhs) return;
+  const bool act_a = !(A.done && A.done[ra]);
+  const bool has_b = ra + 1 < A.nrhs;
+  const bool act_b = has_b && !(A.done && A.done[ra + 1]);
+  if (!act_a && !act_b) return;
+  const Geom &g = A.eg.g;
+  const int p = A.eg.p;
+  const int qoff = (1 - p) * g.Vh;
+  // epilogue coefficients per spin: out = D1 (c [g5] hop) + D2 aux with
+  // D = alpha + i beta g5; c and the optional g5 folded into D1
+  float a1[4], b1[4], a2[4], b2[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const float g5 = s < 2 ? 1.f : -1.f;
+    const float gh = G5HOP ? g5 : 1.f;
+    a1[s] = (float)(A.c * A.d1a) * gh;
+    b1[s] = (float)(A.c * A.d1b) * g5 * gh;
+    a2[s] = (float)A.d2a;
+    b2[s] = (float)A.d2b * g5;
+  }
+  for (int sb = blockIdx.y; sb * (int)blockDim.x < g.Vh; sb += gridDim.y) {
+    const int i = sb * blockDim.x + threadIdx.x;
+    float2 n2 = make_float2(0.f, 0.f);  // |out|^2 of this site, rhs a and b
+    if (i < g.Vh) {
+      const SiteCoord cd = site_coord(g, p, i);
+      const int self = p * g.Vh + i;
+      SpinorPair acc;
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc.c[s][c].re = acc.c[s][c].im = make_float2(0.f, 0.f);
+      hop_pair_dir<3>(acc, A, cd, pr, self, qoff, G5IN);
+      hop_pair_dir<2>(acc, A, cd, pr, self, qoff, G5IN);
+      hop_pair_dir<1>(acc, A, cd, pr, self, qoff, G5IN);
+      hop_pair_dir<0>(acc, A, cd, pr, self, qoff, G5IN);
+      SpinorPair o;
+      diag_pair(o, acc, a1, b1, false);
+      if (AUX) diag_pair(o, A.aux.load_pair(pr, i), a2, b2, true);
+      if (RUPD) {
+        const float2 na = make_float2(-(float)A.alpha[ra], has_b ? -(float)A.alpha[ra + 1] : 0.f);
+        SpinorPair rv = A.rup.load_pair(pr, i);
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            rv.c[s][c].re = __ffma2_rn(na, o.c[s][c].re, rv.c[s][c].re);
+            rv.c[s][c].im = __ffma2_rn(na, o.c[s][c].im, rv.c[s][c].im);
+          }
+        if (A.dot_part) n2 = norm2_pair(rv);
+        store_active(A.rup, pr, i, rv, act_a, act_b);
+      } else {
+        if (A.dot_part) n2 = norm2_pair(o);
+        store_active(A.out, pr, i, o, act_a, act_b);
+      }
+    }
+    if (A.dot_part) {  // the whole warp is here: one row, warp-aligned block width
+      double da = n2.x, db = n2.y;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        da += __shfl_down_sync(0xffffffffu, da, o);
+        db += __shfl_down_sync(0xffffffffu, db, o);
+      }
+      if ((threadIdx.x & 31) == 0) {
+        const int w = sb * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        A.dot_part[(size_t)ra * A.dot_np + w] = da;
+        if (has_b) A.dot_part[(size_t)(ra + 1) * A.dot_np + w] = db;
+      }
+    }
+  }
+}
+
+// ---- pair reductions: blockIdx.y = pair, both right-hand sides at once -----
+// F: __device__ double2 operator()(int pr, int s, bool act_a, bool act_b)
+// E: __device__ void operator()(int r, double total)
+// skip[r] != 0 leaves rhs r out (its lane is neither updated nor reported).
+template <class F, class E>
+__global__ void __launch_bounds__(kRedThreads)
+    k_reduce_pair(F f, E e, int nsites, int nrhs, double *partials, unsigned *counters,
+                  const int *__restrict__ skip) {
+  const int pr = blockIdx.y;
+  const int ra = 2 * pr;
+  const bool has_b = ra + 1 < nrhs;
+  const bool act_a = !(skip && skip[ra]);
+  const bool act_b = has_b && !(skip && skip[ra + 1]);
+  if (!act_a && !act_b) return;
+  __shared__ double sh[2][kRedThreads / 32];
+  __shared__ bool last;
+  double v[2] = {0.0, 0.0};
+  for (int s = blockIdx.x * kRedThreads + threadIdx.x; s < nsites; s += gridDim.x * kRedThreads) {
+    const double2 t = f(pr, s, act_a, act_b);
+    v[0] += t.x;
+    v[1] += t.y;
+  }
+  block_sum<2>(v, sh);
+  double *pa = partials + (size_t)ra * kMaxRedBlocks;
+  double *pb = pa + kMaxRedBlocks;
+  if (threadIdx.x == 0) {
+    pa[blockIdx.x] = v[0];
+    if (has_b) pb[blockIdx.x] = v[1];
+    __threadfence();
+    last = atomicAdd(counters + pr, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  v[0] = v[1] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += kRedThreads) {
+    v[0] += __ldcg(pa + b);
+    if (has_b) v[1] += __ldcg(pb + b);
+  }
+  block_sum<2>(v, sh);
+  if (threadIdx.x == 0) {
+    counters[pr] = 0;
+    if (act_a) e(ra, v[0]);
+    if (act_b) e(ra + 1, v[1]);
+  }
+}
+
+}  // namespace cvcb

@@ -32,6 +32,7 @@
 
 #include "cvcb_internal.h"
 #include "eo_kernels.cuh"
+#include "pair_kernels.cuh"
 #include "reduce.cuh"
 
 namespace cvcb {
@@ -39,6 +40,8 @@ namespace cvcb {
 namespace {
 
 constexpr int kMaxBatch = 24;
+// Tuner keys of the pair-tiled FP32 fields: precision + kPairKey.
+constexpr int kPairKey = 10;
 constexpr size_t kMaxStagedSmem = 200 * 1024;  // opt-in dynamic shared memory of the staged stencil
 
 // ---- batched reductions: blockIdx.y = right-hand side ----------------------
@@ -201,6 +204,35 @@ __global__ void k_p_upd(SF p, SF rs, XF xs, Scal S, int nsites, int nrhs) {
     }
   xs.store(r, s, xv);
   p.store(r, s, pv);
+}
+
+// Pair-tiled form of the CG vector update (thread = site x rhs pair, packed
+// FP32x2 arithmetic; an inactive right-hand side keeps its values).  The
+// residual update r -= alpha A p runs inside the last stencil sweep.
+// x_s += alpha p; p = r_s + beta p
+__global__ void k_p_upd_pt(P32 p, P32 rs, P32 xs, Scal S, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ra = 2 * blockIdx.y;
+  if (s >= nsites) return;
+  const bool act_a = !S.done[ra];
+  const bool act_b = ra + 1 < nrhs && !S.done[ra + 1];
+  if (!act_a && !act_b) return;
+  const float2 a = make_float2((float)S.alpha[ra], act_b ? (float)S.alpha[ra + 1] : 0.f);
+  const float2 b = make_float2((float)S.beta[ra], act_b ? (float)S.beta[ra + 1] : 0.f);
+  const SpinorPair rv = rs.load_pair(blockIdx.y, s);
+  SpinorPair pv = p.load_pair(blockIdx.y, s);
+  SpinorPair xv = xs.load_pair(blockIdx.y, s);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      xv.c[k][c].re = __ffma2_rn(a, pv.c[k][c].re, xv.c[k][c].re);
+      xv.c[k][c].im = __ffma2_rn(a, pv.c[k][c].im, xv.c[k][c].im);
+      pv.c[k][c].re = __ffma2_rn(b, pv.c[k][c].re, rv.c[k][c].re);
+      pv.c[k][c].im = __ffma2_rn(b, pv.c[k][c].im, rv.c[k][c].im);
+    }
+  store_active(xs, blockIdx.y, s, xv, act_a, act_b);
+  store_active(p, blockIdx.y, s, pv, act_a, act_b);
 }
 
 // Reliable update, step 1: x64 += x_s / scale; x_s = 0 (rhs with skip[r] == 0)
@@ -459,11 +491,14 @@ template <> constexpr double link_bytes<L64>() { return 144; }
 template <> constexpr double link_bytes<L32f>() { return 72; }
 template <> constexpr double link_bytes<L32c>() { return 48; }
 template <> constexpr double link_bytes<L16c>() { return 24; }
+template <> constexpr double link_bytes<LT32f>() { return 72; }
+template <> constexpr double link_bytes<LT32c>() { return 48; }
 template <class SF>
 constexpr double spinor_bytes();
 template <> constexpr double spinor_bytes<F64Acc>() { return 192; }
 template <> constexpr double spinor_bytes<F32Acc>() { return 96; }
 template <> constexpr double spinor_bytes<F16Acc>() { return 52; }  // 48 + float norm
+template <> constexpr double spinor_bytes<P32>() { return 96; }
 
 int red_blocks_sites(int n) {
   int b = (n + kRedThreads * 2 - 1) / (kRedThreads * 2);
@@ -541,13 +576,17 @@ struct Batch {
       CVCB_CUDA(cudaEventRecordWithFlags(rec.a, L->stream, capturing ? cudaEventRecordExternal : 0));
     }
     bool packed = false;
-    if constexpr (sizeof(typename AF::R) == 4) {
+    if constexpr (std::is_same<AF, P32>::value) {  // pair-tiled fields
+      k_eo_hop_pt<LL, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
+      packed = true;
+    } else if constexpr (sizeof(typename AF::R) == 4) {
       if (sh.pk) {  // two rhs per thread in packed FP32x2 arithmetic
         k_eo_hop_x2<AF, LL, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
         packed = true;
       }
     }
-    if (packed) {
+    if constexpr (std::is_same<AF, P32>::value) {
+    } else if (packed) {
     } else if (by > 1 && sh.nr == 1) {
       // rows of the block share links staged in shared memory
       auto kern = [] {
@@ -589,6 +628,48 @@ struct Batch {
     return CVCB_OK;
   }
 
+  // The last sweep of M^+M on pair-tiled fields, fused with the residual
+  // update of CG: r_s -= alpha (A(-mu) yo + 1/2 g5 H_oe te2) and per-warp
+  // partials of |r_s|^2 (A p itself is not stored)
+  int hop_rupd(SF in, SF aux, double d2a, double d2b) {
+    if constexpr (std::is_same<SF, P32>::value) {
+      HopArgs<SF, LF> a{rs, in, aux, links, EoGeom{g, 1}, n, S.done, 1, 0, d2a, d2b, 0.5};
+      if (!dot_fusable()) {
+        set_error("fused residual update needs warp-aligned blocks");
+        return CVCB_ERR_STATE;
+      }
+      a.dot_part = dot_part;
+      a.dot_np = ((g.Vh + shape.bx - 1) / shape.bx) * (shape.bx / 32);
+      dot_np = a.dot_np;
+      a.rup = rs;
+      a.alpha = S.alpha;
+      const int groups = (n + 1) / 2;
+      const int by = std::min(shape.by, groups);
+      const int site_blocks = (g.Vh + shape.bx - 1) / shape.bx;
+      dim3 block(shape.bx, by), grid((groups + by - 1) / by, std::min(site_blocks, 65535));
+      Rec rec{};
+      if (prof_rec) {
+        CVCB_CUDA(cudaEventCreate(&rec.a));
+        CVCB_CUDA(cudaEventCreate(&rec.b));
+        CVCB_CUDA(cudaEventRecordWithFlags(rec.a, L->stream, capturing ? cudaEventRecordExternal : 0));
+      }
+      k_eo_hop_pt<LF, false, true, true, true><<<grid, block, 0, L->stream>>>(a);
+      CVCB_LAUNCHED(L);
+      if (prof_rec) {
+        CVCB_CUDA(cudaEventRecordWithFlags(rec.b, L->stream, capturing ? cudaEventRecordExternal : 0));
+        // neighbours, aux, r read and r written
+        rec.bytes_per_rhs = (double)g.Vh * spinor_bytes<SF>() * 4;
+        rec.link_bytes = 4.0 * g.V * link_bytes<LF>();
+        recs.push_back(rec);
+      }
+      return CVCB_OK;
+    } else {
+      (void)in, (void)aux, (void)d2a, (void)d2b;
+      set_error("fused residual update needs pair-tiled fields");
+      return CVCB_ERR_STATE;
+    }
+  }
+
   // diagonal coefficients
   double ka() const { return 0.5 / kap; }
   void ainv(double m, double &a, double &b) const {
@@ -623,6 +704,26 @@ struct Batch {
 
   // one CG iteration (sloppy)
   int iteration() {
+    if constexpr (std::is_same<SF, P32>::value) {
+      // pair-tiled fields: alpha = |r|^2 / |M p|^2 between the two
+      // applications of M, and the last sweep updates r itself
+      const int np = (n + 1) / 2;
+      double ia, ib, ja, jb;
+      ainv(mu, ia, ib);
+      ainv(-mu, ja, jb);
+      CVCB_TRY((hop<SF, LF, false, false, false>(te, p, p, links, 0, S.done, ia, ib, 0, 0, -0.5)));
+      CVCB_TRY((hop<SF, LF, false, false, true>(yo, te, p, links, 1, S.done, 1, 0, ka(), mu, 0.5,
+                                                dot_part)));
+      k_dot_finish<<<n, kRedThreads, 0, L->stream>>>(dot_part, dot_np, EpiAlphaB{S}, S.done);
+      CVCB_LAUNCHED(L);
+      CVCB_TRY((hop<SF, LF, true, false, false>(te2, yo, yo, links, 0, S.done, ja, jb, 0, 0, -0.5)));
+      CVCB_TRY(hop_rupd(te2, yo, ka(), -mu));
+      k_dot_finish<<<n, kRedThreads, 0, L->stream>>>(dot_part, dot_np, EpiBetaB{S}, S.done);
+      CVCB_LAUNCHED(L);
+      k_p_upd_pt<<<dim3((g.Vh + 127) / 128, np), 128, 0, L->stream>>>(p, rs, xs, S, g.Vh, n);
+      CVCB_LAUNCHED(L);
+      return CVCB_OK;
+    }
     dim3 rg(red_blocks_sites(g.Vh), n);
     if (dot_fusable()) {
       CVCB_TRY(normal_op_sloppy(Ap, p, S.done, dot_part));
@@ -701,6 +802,10 @@ template <>
 F64Acc make_sloppy<F64Acc>(void *base, size_t Vh, int, float *) {
   return F64Acc{static_cast<double2 *>(base), Vh, 12 * Vh};
 }
+template <>
+P32 make_sloppy<P32>(void *base, size_t Vh, int, float *) {
+  return P32{static_cast<float4 *>(base), p32_pair_float4((int)Vh)};
+}
 
 template <class SF>
 size_t sloppy_site_bytes();
@@ -710,6 +815,16 @@ template <>
 size_t sloppy_site_bytes<F16Acc>() { return 48; }
 template <>
 size_t sloppy_site_bytes<F64Acc>() { return 192; }
+template <>
+size_t sloppy_site_bytes<P32>() { return 96; }
+
+// Bytes of one sloppy field set of n right-hand sides (pair-tiled sets hold
+// whole pairs of whole tiles).
+template <class SF>
+size_t sloppy_field_bytes(size_t Vh, int n) {
+  if (std::is_same<SF, P32>::value) return p32_pair_float4((int)Vh) * sizeof(float4) * ((n + 1) / 2);
+  return sloppy_site_bytes<SF>() * Vh * n;
+}
 
 template <class LF>
 LF make_links(cvcb_lattice *L);
@@ -739,6 +854,16 @@ L32f make_links<L32f>(cvcb_lattice *L) {
   return l;
 }
 template <>
+LT32f make_links<LT32f>(cvcb_lattice *L) {
+  return LT32f{L->UT32f, {}};
+}
+template <>
+LT32c make_links<LT32c>(cvcb_lattice *L) {
+  LT32c l{L->UT32c, {}};
+  for (int m = 0; m < 4; ++m) l.ph[m] = phase_cubed(L, m);
+  return l;
+}
+template <>
 L16c make_links<L16c>(cvcb_lattice *L) {
   L16c l{L->U16c, (size_t)L->g.V, {}};
   for (int m = 0; m < 4; ++m) l.ph[m] = phase_cubed(L, m);
@@ -763,8 +888,8 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   B.links64 = make_links<L64>(L);
   // one FP64 full field set (none when only the sloppy stencil is timed)
   const size_t f64 = with_fp64 ? (size_t)12 * g.V * sizeof(double2) * n : 0;
-  const size_t sl = sloppy_site_bytes<SF>() * (size_t)g.Vh * n;
-  const size_t xsl = sloppy_site_bytes<XF>() * (size_t)g.Vh * n;
+  const size_t sl = sloppy_field_bytes<SF>(g.Vh, n);
+  const size_t xsl = sloppy_field_bytes<XF>(g.Vh, n);
   const size_t nrm = sizeof(float) * (size_t)g.Vh * n;
   auto rnd = [](size_t b) { return (b + 255) & ~size_t(255); };  // every piece 256-aligned
   const size_t scal = 8 * rnd(sizeof(double) * kMaxBatch) + 3 * rnd(sizeof(int) * kMaxBatch);
@@ -853,7 +978,8 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
     B.shape = LaunchShape{block_threads, 1, 1};
     return CVCB_OK;
   }
-  auto key = std::make_tuple(L->g.V, prec, recon, B.n);
+  constexpr bool pairs = std::is_same<SF, P32>::value;
+  auto key = std::make_tuple(L->g.V, prec + (pairs ? kPairKey : 0), recon, B.n);
   auto it = g_tuned_shape.find(key);
   if (it != g_tuned_shape.end()) {
     B.shape = it->second;
@@ -868,6 +994,7 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
         f.bx * f.by <= kHopMaxThreads) {
       if (nf < 4 || f.nr != 2) f.pk = 0;
       if (sizeof(typename SF::R) == 8) f.nr = 1, f.pk = 0;
+      if (pairs) f.nr = 2, f.pk = 1;  // pair-tiled fields: one rhs pair per thread
       B.shape = f;
       g_tuned_shape[key] = f;
       return CVCB_OK;
@@ -886,6 +1013,7 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
     for (int by : bys) {
       const int nr = np[0];
       if (fp64 && nr > 1) continue;
+      if (pairs && !(nr == 2 && np[1] == 1)) continue;
       if (nr > B.n || by * nr > B.n || bx * by > kHopMaxThreads || bx * by < 32) continue;
       B.shape.bx = bx;
       B.shape.by = by;
@@ -1214,7 +1342,7 @@ int time_stencil_t(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int
   Batch<SF, XF, LF> B;
   CVCB_TRY(setup_batch(L, B, nrhs, /*with_fp64=*/false));
   // zero contents: timing of the stencil does not depend on the values
-  CVCB_CUDA(cudaMemsetAsync(B.p.p, 0, sloppy_site_bytes<SF>() * (size_t)L->g.Vh * nrhs, L->stream));
+  CVCB_CUDA(cudaMemsetAsync(B.p.p, 0, sloppy_field_bytes<SF>(L->g.Vh, nrhs), L->stream));
   CVCB_CUDA(cudaMemsetAsync(B.S.done, 0, sizeof(int) * nrhs, L->stream));
   CVCB_TRY(tune_shape(L, B, prec, recon));
   double ia, ib;
@@ -1243,6 +1371,16 @@ int time_stencil_t(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int
 }
 
 }  // namespace
+
+// FP32 inner iterations on pair-tiled fields (k_eo_hop_pt and the pair CG
+// kernels) instead of per-rhs fields: CVCB_PAIRS=1 (read once).
+bool use_pairs() {
+  static const bool on = [] {
+    const char *e = getenv("CVCB_PAIRS");
+    return e && atoi(e) != 0;
+  }();
+  return on;
+}
 
 int time_stencil(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int reps, double *ms) {
   if (!L->have_gauge) {
@@ -1277,6 +1415,9 @@ int time_stencil(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int r
   }
   if (prec == CVCB_PREC_DOUBLE)
     return time_stencil_t<F64Acc, F64Acc, L64>(L, kind, prec, 18, nrhs, reps, ms);
+  if (prec == CVCB_PREC_SINGLE && use_pairs())
+    return recon == 12 ? time_stencil_t<P32, P32, LT32c>(L, kind, prec, recon, nrhs, reps, ms)
+                       : time_stencil_t<P32, P32, LT32f>(L, kind, prec, recon, nrhs, reps, ms);
   if (prec == CVCB_PREC_SINGLE)
     return recon == 12 ? time_stencil_t<F32Acc, F32Acc, L32c>(L, kind, prec, recon, nrhs, reps, ms)
                        : time_stencil_t<F32Acc, F32Acc, L32f>(L, kind, prec, recon, nrhs, reps, ms);
@@ -1298,7 +1439,7 @@ int tune_batch(cvcb_lattice *L, const cvcb_solver_params *P, int recon, int nrhs
     if (n > kMaxBatch || (n > nrhs && n != cands[0])) continue;
     Batch<SF, XF, LF> B;
     CVCB_TRY(setup_batch(L, B, n, /*with_fp64=*/false));
-    CVCB_CUDA(cudaMemsetAsync(B.p.p, 0, sloppy_site_bytes<SF>() * (size_t)L->g.Vh * n, L->stream));
+    CVCB_CUDA(cudaMemsetAsync(B.p.p, 0, sloppy_field_bytes<SF>(L->g.Vh, n), L->stream));
     CVCB_TRY(tune_shape(L, B, P->precision, recon, P->block_threads));
     float ms;
     if (time_ms(L, [&] { return B.normal_op_sloppy(B.Ap, B.p, nullptr); }, 3, &ms) != CVCB_OK) {
@@ -1410,7 +1551,8 @@ int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int
   std::memset(st, 0, sizeof *st);
   int nb = P->block_rhs;
   if (!nb) {
-    auto key = std::make_tuple(L->g.V, P->precision, recon, nrhs);
+    const bool pairs = P->precision == CVCB_PREC_SINGLE && use_pairs();
+    auto key = std::make_tuple(L->g.V, P->precision + (pairs ? kPairKey : 0), recon, nrhs);
     auto it = g_tuned_batch.find(key);
     if (it != g_tuned_batch.end()) {
       nb = it->second;
@@ -1418,6 +1560,9 @@ int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int
       int rc;
       if (P->precision == CVCB_PREC_DOUBLE)
         rc = tune_batch<F64Acc, F64Acc, L64>(L, P, recon, nrhs, &nb);
+      else if (pairs)
+        rc = recon == 12 ? tune_batch<P32, P32, LT32c>(L, P, recon, nrhs, &nb)
+                         : tune_batch<P32, P32, LT32f>(L, P, recon, nrhs, &nb);
       else if (P->precision == CVCB_PREC_SINGLE)
         rc = recon == 12 ? tune_batch<F32Acc, F32Acc, L32c>(L, P, recon, nrhs, &nb)
                          : tune_batch<F32Acc, F32Acc, L32f>(L, P, recon, nrhs, &nb);
@@ -1432,6 +1577,9 @@ int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int
   auto run = [&](double *const *xs, const double *const *bs, int n, cudaEvent_t read) {
     if (P->precision == CVCB_PREC_DOUBLE)
       return run_batch<F64Acc, F64Acc, L64>(L, xs, bs, n, P, st, nullptr, read);
+    if (P->precision == CVCB_PREC_SINGLE && use_pairs())
+      return recon == 12 ? run_batch<P32, P32, LT32c>(L, xs, bs, n, P, st, nullptr, read)
+                         : run_batch<P32, P32, LT32f>(L, xs, bs, n, P, st, nullptr, read);
     if (P->precision == CVCB_PREC_SINGLE)
       return recon == 12 ? run_batch<F32Acc, F32Acc, L32c>(L, xs, bs, n, P, st, nullptr, read)
                          : run_batch<F32Acc, F32Acc, L32f>(L, xs, bs, n, P, st, nullptr, read);
@@ -1493,7 +1641,9 @@ int cvcb_tuned_shape(cvcb_lattice *L, int precision, int link_recon, int nrhs, i
                      int *rows_per_block, int *rhs_per_thread, int *variant) {
   if (!L || !sites_per_block || !rows_per_block || !rhs_per_thread || !variant)
     return CVCB_ERR_NULL;
-  auto it = cvcb::g_tuned_shape.find(std::make_tuple(L->g.V, precision, link_recon, nrhs));
+  const bool pairs = precision == CVCB_PREC_SINGLE && cvcb::use_pairs();
+  auto it = cvcb::g_tuned_shape.find(std::make_tuple(
+      L->g.V, precision + (pairs ? cvcb::kPairKey : 0), link_recon, nrhs));
   if (it == cvcb::g_tuned_shape.end()) {
     cvcb::set_error("no tuned shape for this configuration yet");
     return CVCB_ERR_STATE;
@@ -1502,7 +1652,7 @@ int cvcb_tuned_shape(cvcb_lattice *L, int precision, int link_recon, int nrhs, i
   *sites_per_block = s.bx;
   *rows_per_block = s.by;
   *rhs_per_thread = s.nr;
-  *variant = s.pk ? 2 : (s.by > 1 && s.nr == 1) ? 1 : 0;
+  *variant = pairs ? 3 : s.pk ? 2 : (s.by > 1 && s.nr == 1) ? 1 : 0;
   return CVCB_OK;
 }
 

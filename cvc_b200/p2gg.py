@@ -41,11 +41,14 @@ def shifted_sites(dims, site):
 
 
 def p2gg(lat, source_site, dt, momentum, gamma_id, propagator_position=0, params=None,
-         device="cuda"):
+         device="cuda", keep=None):
     """Pi_mu_nu(x) of the P -> gamma gamma three-point function for the source
     at lexicographic site `source_site`; returns (conn, contact, stats) with
     conn the 32*V doubles of the reference layout (a torch CUDA tensor) and
-    stats a dict of solve counts and times."""
+    stats a dict of solve counts and times.  With a dict `keep`, the first
+    forward up column ("up0"), its sequential source ("seq_source0") and the
+    120 contracted columns ("fields": sequential propagators, then dn) are
+    left in it for checks."""
     import torch
     if params is None:
         params = solver_defaults()
@@ -82,8 +85,13 @@ def p2gg(lat, source_site, dt, momentum, gamma_id, propagator_position=0, params
     # sequential sources from the up columns (the point sources are not needed
     # any more: their storage takes the sequential sources)
     t_seq = (source_site // (lat.LX * lat.LY * lat.LZ) + dt) % lat.T
+    if keep is not None:
+        keep["up0"] = up[0].clone()
     for i in range(60):
         lat.p2gg_seq_source(src[i], up[i], t_seq, momentum, gamma_id, propagator_position)
+    if keep is not None:
+        keep["seq_source0"] = src[0].clone()
+        keep["t_seq"] = t_seq
     # the sequential propagators replace the up columns
     solve(up, src, mu if propagator_position == 0 else -mu)
     lat.set_params(kappa, mu, bc)
@@ -95,6 +103,8 @@ def p2gg(lat, source_site, dt, momentum, gamma_id, propagator_position=0, params
     conn, contact = lat.cvc_contract(up + dn, source_site, conn=conn)
     torch.cuda.synchronize()
     stats["contract_s"] = time.perf_counter() - t0
+    if keep is not None:
+        keep["fields"] = up + dn
     return conn, contact, stats
 
 

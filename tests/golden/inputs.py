@@ -39,3 +39,30 @@ def gauge(seed, V):
     r2 = np.conj(np.cross(r0, r1))
     out = np.stack([r0, r1, r2], axis=1)
     return np.stack([out.real, out.imag], axis=-1).reshape(72 * V).copy()
+
+
+def neighbours(dims, site):
+    """The 8 nearest neighbours of a site (lexicographic)."""
+    T, LX, LY, LZ = dims
+    t, r = divmod(site, LX * LY * LZ)
+    x, r = divmod(r, LY * LZ)
+    y, z = divmod(r, LZ)
+    c, L = [t, x, y, z], [T, LX, LY, LZ]
+    out = []
+    for m in range(4):
+        for d in (1, -1):
+            cc = list(c)
+            cc[m] = (cc[m] + d) % L[m]
+            out.append(((cc[0] * LX + cc[1]) * LY + cc[2]) * LZ + cc[3])
+    return out
+
+
+def sample_sites(dims, site, n, seed=2024):
+    """The source, its 8 neighbours, then n distinct further sites (numpy
+    PCG64 stream `seed`), sorted after the first 9."""
+    V = int(np.prod(dims))
+    head = [site] + neighbours(dims, site)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rest = rng.choice(V, size=n + 64, replace=False)
+    rest = np.sort(np.array([s for s in rest if s not in head][:n]))
+    return np.concatenate([np.array(head), rest]).astype(np.int64)

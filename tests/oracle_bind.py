@@ -162,6 +162,38 @@ class Oracle:
         self.lib.orc_cvc_contract(ctypes.byref(self.L), arr, src, _p(conn), _p(contact))
         return conn, contact
 
+    def cvc_contract_sites(self, sites, src, fetch):
+        """Pi_mu_nu at the lexicographic `sites` only, and the contact term,
+        for lattices whose 120 full fields would not fit the host.  Pi(x)
+        reads the fields at x and x + mu-hat and the links at x (the contact
+        term the fields at the source and source + nu-hat), so the oracle's
+        own contraction runs unchanged on a compact lattice made of those
+        sites: the same per-site arithmetic, with the neighbour table and the
+        links restricted to them.  `fetch(idx)` returns the 120 columns at
+        the lexicographic sites idx, each an array of shape (len(idx), 24).
+        Returns (pi of shape (len(sites), 32), contact)."""
+        iup = np.ctypeslib.as_array(self.L.iup, shape=(4 * self.V,)).reshape(-1, 4)
+        need = sorted(set(int(x) for x in sites) | {int(src)})
+        G = np.array(sorted(set(need) | set(iup[need].ravel().tolist())), np.int64)
+        pos = {int(x): i for i, x in enumerate(G)}
+        iup_c = np.zeros((len(G), 4), np.int32)  # sites outside `need` point at row 0
+        for x in need:
+            iup_c[pos[x]] = [pos[int(n)] for n in iup[x]]
+        gauge_c = np.ascontiguousarray(self._gauge.reshape(-1, 72)[G])
+        rows = [np.ascontiguousarray(r, np.float64) for r in fetch(G)]
+        assert len(rows) == 120 and all(r.shape == (len(G), 24) for r in rows)
+        Lc = OrcLattice()
+        ctypes.pointer(Lc)[0] = self.L
+        Lc.V = len(G)
+        Lc.iup = iup_c.ctypes.data_as(ctypes.POINTER(_I))
+        Lc.idn = Lc.iup
+        Lc.gauge = gauge_c.ctypes.data_as(ctypes.POINTER(_D))
+        arr = (ctypes.c_void_p * 120)(*[r.ctypes.data for r in rows])
+        conn = np.zeros(32 * len(G))
+        contact = np.zeros(8)
+        self.lib.orc_cvc_contract(ctypes.byref(Lc), arr, pos[int(src)], _p(conn), _p(contact))
+        return conn.reshape(-1, 32)[[pos[int(x)] for x in sites]], contact
+
     def cvc_ward(self, conn):
         wi = np.zeros(8 * self.V)
         self.lib.orc_cvc_ward(ctypes.byref(self.L), _p(np.ascontiguousarray(conn)), _p(wi))

@@ -1,0 +1,107 @@
+"""Pi_mu_nu at the reference's own configuration against the reference:
+8^3x16, kappa 0.150, 2 kappa mu 0.01, gauge U = exp(i 0.3 H) of ranlxd seed
+1234, antiperiodic in time, source at the origin.
+
+tests/golden/reference_c1.npz holds the unmodified reference's output
+(tests/golden/make_golden_configs.py): its invert_Qtm_her solved all 120
+columns (both flavours, point sources at y + mu-hat and y, 12 spin-colour
+components) to a relative residual of 1e-13, and its cvc_exact2_xspace
+program contracted them (cvc_exact2_xspace.c:577-861), printing the contact
+term.  Here the batched solver computes the same 120 columns -- with FP64,
+FP32 and FP16+norm inner iterations, FP64 reliable updates, relative
+residual 1e-12 -- and the GPU contraction turns them into Pi.  Pi and the
+contact term must agree with the reference's to 1e-10 relative (largest
+component difference over the largest |Pi|), and the Ward identity of the
+GPU's Pi must hold: the divergence vanishes except at y and y + nu, where
+it is +- the reference's contact term.  The FP64 mirror of invert_Qtm_her
+needs the reference's iteration counts within 10 %.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FIX = os.path.join(ROOT, "tests", "golden", "reference_c1.npz")
+
+
+@pytest.fixture(scope="module")
+def c1(cb):
+    fix = np.load(FIX)
+    dims = tuple(int(d) for d in fix["cfg_dims"])
+    kappa = float(fix["cfg_kappa"])
+    mu = float(fix["cfg_two_kappa_mu"]) / (2 * kappa)
+    g = cb.gauge_random(*dims, float(fix["cfg_eps"]), int(fix["cfg_seed"]))
+    lat = cb.Lattice(*dims, kappa=kappa, mu=mu)
+    lat.upload_gauge(g)
+    yield lat, fix, dims, kappa, mu
+    lat.close()
+
+
+def columns(dims, src):
+    from cvc_b200.p2gg import shifted_sites
+    V = int(np.prod(dims))
+    bs = []
+    for s in shifted_sites(dims, src):
+        for sc in range(12):
+            b = np.zeros(24 * V)
+            b[24 * s + 2 * sc] = 1.0
+            bs.append(b)
+    return bs
+
+
+def test_c1_gauge_matches_fixture(c1):
+    lat, fix, *_ = c1
+    assert abs(lat.plaquette()[0] - float(fix["plaquette"])) < 1e-14
+
+
+@pytest.mark.parametrize("prec", [0, 1, 2], ids=["fp64", "fp32-inner", "fp16-inner"])
+def test_c1_pi_against_reference(cb, c1, prec):
+    lat, fix, dims, kappa, mu = c1
+    V = lat.VOLUME
+    src = int(fix["cfg_source"])
+    bs = columns(dims, src)
+    p = cb.solver_defaults()
+    p.precision = prec
+    p.link_recon = 18 if prec == 0 else 12
+    p.tol = 1e-12
+    fields = []
+    for m in (mu, -mu):
+        lat.set_params(kappa, m)
+        xs = [np.zeros(24 * V) for _ in bs]
+        st = lat.solve(xs, bs, p)
+        assert st.converged == 60 and st.max_true_res <= 1e-12
+        fields += xs
+    lat.set_params(kappa, mu)
+    conn, contact = lat.cvc_contract(fields, src)
+    assert rel_err(conn, fix["pi"]) < 1e-10
+    assert rel_err(contact, fix["contact"]) < 1e-10
+    # Ward identity of the GPU's Pi, with the reference's contact term
+    wi = lat.cvc_ward(conn).reshape(V, 4, 2)
+    from cvc_b200.p2gg import shifted_sites
+    shifted = shifted_sites(dims, src)
+    scale = np.max(np.abs(conn))
+    for nu in range(4):
+        w = wi[:, nu, 0] + 1j * wi[:, nu, 1]
+        ct = fix["contact"][2 * nu] + 1j * fix["contact"][2 * nu + 1]
+        assert abs(w[src] - ct) < 1e-9 * scale
+        assert abs(w[shifted[nu]] + ct) < 1e-9 * scale
+        assert np.max(np.delete(np.abs(w), [src, shifted[nu]])) < 1e-9 * scale
+
+
+def test_c1_fp64_mirror_iterations(c1):
+    """The GPU's FP64 invert_Qtm_her takes the reference's iteration count
+    (within 10 %) on the unshifted up columns 0, 5 and 11."""
+    lat, fix, dims, kappa, mu = c1
+    V = lat.VOLUME
+    src = int(fix["cfg_source"])
+    bs = columns(dims, src)
+    lat.set_params(kappa, mu)
+    for k in (48, 53, 59):  # the unshifted source is the fifth shift
+        x = np.zeros(24 * V)
+        n = lat.invert_Qtm_her(x, bs[k], float(fix["cfg_precision"]), 20000)
+        nref = int(fix["iterations"][k])
+        assert n > 0 and abs(n - nref) <= max(3, nref // 10), (k, n, nref)
