@@ -309,8 +309,11 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     T, LX, LY, LZ = DIMS
+    from cvc_b200 import sharding
     lat = cb.Lattice(*DIMS, device=local, kappa=KAPPA, mu=MU, bc_angle=(1.0, 0.0, 0.0, 0.0))
-    gauge = cb.gauge_random(*DIMS, EPS, SEED)
+    # the gauge field is made on rank 0 and broadcast (one collective, untimed)
+    gauge = sharding.broadcast_field(cb.gauge_random(*DIMS, EPS, SEED) if rank == 0 else None,
+                                     72 * T * LX * LY * LZ, torch.device("cuda", local))
     lat.upload_gauge(gauge)
     V = lat.VOLUME
     sites = source_sites(rank, cb.ranlxd)
@@ -403,12 +406,14 @@ def main():
             "stencil_shape": {"sites_per_block": shape[0].value, "rows_per_block": shape[1].value,
                               "rhs_per_thread": shape[2].value,
                               "variant": ["per-thread links", "shared-memory links",
-                                          "packed FP32x2 rhs pairs"][shape[3].value]},
+                                          "packed FP32x2 rhs pairs",
+                                          "pair-tiled fields"][shape[3].value]},
             "inner_iterations_per_step": iters // max(args.steps, 1),
             "max_true_residual": worst_res,
         },
         "roofline": {
-            "kernel": ["k_eo_hop", "k_eo_hop_staged", "k_eo_hop_x2"][shape[3].value] +
+            "kernel": ["k_eo_hop", "k_eo_hop_staged", "k_eo_hop_x2",
+                       "k_eo_hop_pt"][shape[3].value] +
                       " (batched even/odd stencil sweep, "
                       f"{args.precision}, {params.link_recon}-real links)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

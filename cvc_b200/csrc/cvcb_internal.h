@@ -285,6 +285,8 @@ int pi_backward(cvcb_lattice *L, const double *wts, double *dLdU, double *dLdmu,
 
 // solver_mixed.cu
 int time_stencil(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int reps, double *ms);
+int sloppy_normal_op(cvcb_lattice *L, int prec, int recon, int layout, int n,
+                     const double *const *in, double *const *out);
 int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int nrhs,
                   const cvcb_solver_params *p, cvcb_solver_stats *st);
 

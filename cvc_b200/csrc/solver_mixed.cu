@@ -39,7 +39,9 @@ namespace cvcb {
 
 namespace {
 
-constexpr int kMaxBatch = 24;
+// Right-hand sides per batch: up to 96, so that the 8 x 12 columns of the
+// benchmark can advance as one set (each link loaded once per site for all).
+constexpr int kMaxBatch = 96;
 // Tuner keys of the pair-tiled FP32 fields: precision + kPairKey.
 constexpr int kPairKey = 10;
 constexpr size_t kMaxStagedSmem = 200 * 1024;  // opt-in dynamic shared memory of the staged stencil
@@ -311,6 +313,15 @@ __global__ void k_to_sloppy(SF dst, F64Acc src, const double *scale, const int *
   dst.store(r, s, convert<typename SF::R>(v));
 }
 
+// FP64 <- sloppy (per rhs)
+template <class SF>
+__global__ void k_from_sloppy(F64Acc dst, SF src, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (s >= nsites || r >= nrhs) return;
+  dst.store(r, s, convert<double>(src.load(r, s)));
+}
+
 template <class SF>
 struct RedNormS {
   SF v;
@@ -434,10 +445,10 @@ struct FlagArgs {
   int v[kMaxBatch];
 };
 __global__ void k_put_flags(int *__restrict__ dst, FlagArgs f, int n) {
-  if ((int)threadIdx.x < n) dst[threadIdx.x] = f.v[threadIdx.x];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = f.v[i];
 }
 __global__ void k_fetch(double *__restrict__ dst, const double *__restrict__ src, int n) {
-  if ((int)threadIdx.x < n) dst[threadIdx.x] = src[threadIdx.x];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
 
 constexpr int kMailSlots = 4;  // hb2, rr, rhat2, spare
@@ -445,7 +456,7 @@ constexpr int kMailSlots = 4;  // hb2, rr, rhat2, spare
 int put_flags(cvcb_lattice *L, int *dev, const std::vector<int> &h, int n) {
   FlagArgs f{};
   for (int i = 0; i < n; ++i) f.v[i] = h[i];
-  k_put_flags<<<1, 32, 0, L->stream>>>(dev, f, n);
+  k_put_flags<<<1, 128, 0, L->stream>>>(dev, f, n);
   CVCB_LAUNCHED(L);
   return CVCB_OK;
 }
@@ -458,7 +469,7 @@ int fetch(cvcb_lattice *L, const double *dev, int n, int slot) {
                             sizeof(double) * kMaxBatch * kMailSlots, cudaHostAllocMapped));
     CVCB_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&L->mbox_dev), L->mbox_host, 0));
   }
-  k_fetch<<<1, 32, 0, L->stream>>>(L->mbox_dev + slot * kMaxBatch, dev, n);
+  k_fetch<<<1, 128, 0, L->stream>>>(L->mbox_dev + slot * kMaxBatch, dev, n);
   CVCB_LAUNCHED(L);
   return CVCB_OK;
 }
@@ -1372,6 +1383,56 @@ int time_stencil_t(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int
 
 }  // namespace
 
+namespace {
+// M^+M of the batched solver's inner iterations on n fields (odd sites of
+// CVC-layout FP64 fields in and out; even sites of out are zero).
+template <class SF, class XF, class LF>
+int sloppy_normal_op_t(cvcb_lattice *L, int prec, int recon, int n, const double *const *in,
+                       double *const *out) {
+  Batch<SF, XF, LF> B;
+  CVCB_TRY(setup_batch(L, B, n));
+  CVCB_TRY(tune_shape(L, B, prec, recon, 0));
+  const Geom &g = L->g;
+  const size_t fs = (size_t)12 * g.V;
+  for (int i = 0; i < n; ++i) CVCB_TRY(spinor_in(L, B.b64 + i * fs, in[i], g.V));
+  std::vector<double> ones(kMaxBatch, 1.0);
+  CVCB_CUDA(cudaMemcpyAsync(B.S.scale, ones.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
+                            L->stream));
+  dim3 eg((g.Vh + 127) / 128, n);
+  k_to_sloppy<<<eg, 128, 0, L->stream>>>(B.p, B.f64(B.b64, 1), B.S.scale, nullptr, g.Vh, n);
+  CVCB_LAUNCHED(L);
+  CVCB_TRY(B.normal_op_sloppy(B.Ap, B.p, nullptr));
+  CVCB_CUDA(cudaMemsetAsync(B.y64, 0, fs * n * sizeof(double2), L->stream));
+  k_from_sloppy<<<eg, 128, 0, L->stream>>>(B.f64(B.y64, 1), B.Ap, g.Vh, n);
+  CVCB_LAUNCHED(L);
+  for (int i = 0; i < n; ++i) CVCB_TRY(spinor_out(L, out[i], B.y64 + i * fs, g.V));
+  CVCB_CUDA(cudaStreamSynchronize(L->stream));
+  return CVCB_OK;
+}
+}  // namespace
+
+int sloppy_normal_op(cvcb_lattice *L, int prec, int recon, int layout, int n,
+                     const double *const *in, double *const *out) {
+  if (!L->have_gauge) {
+    set_error("no gauge field uploaded");
+    return CVCB_ERR_STATE;
+  }
+  if (n <= 0 || n > kMaxBatch || prec < 0 || prec > 2 || (recon != 12 && recon != 18) ||
+      layout < 0 || layout > 1 || (layout == 1 && prec != CVCB_PREC_SINGLE)) {
+    set_error("invalid arguments");
+    return CVCB_ERR_ARG;
+  }
+  if (prec == CVCB_PREC_DOUBLE) return sloppy_normal_op_t<F64Acc, F64Acc, L64>(L, prec, 18, n, in, out);
+  if (layout == 1)
+    return recon == 12 ? sloppy_normal_op_t<P32, P32, LT32c>(L, prec, recon, n, in, out)
+                       : sloppy_normal_op_t<P32, P32, LT32f>(L, prec, recon, n, in, out);
+  if (prec == CVCB_PREC_SINGLE)
+    return recon == 12 ? sloppy_normal_op_t<F32Acc, F32Acc, L32c>(L, prec, recon, n, in, out)
+                       : sloppy_normal_op_t<F32Acc, F32Acc, L32f>(L, prec, recon, n, in, out);
+  return recon == 12 ? sloppy_normal_op_t<F16Acc, F32Acc, L16c>(L, prec, recon, n, in, out)
+                     : sloppy_normal_op_t<F16Acc, F32Acc, L32f>(L, prec, recon, n, in, out);
+}
+
 // FP32 inner iterations on pair-tiled fields (k_eo_hop_pt and the pair CG
 // kernels) instead of per-rhs fields: CVCB_PAIRS=1 (read once).
 bool use_pairs() {
@@ -1429,14 +1490,25 @@ int time_stencil(cvcb_lattice *L, int kind, int prec, int recon, int nrhs, int r
 // operator is timed (with its own tuned launch shape) for each candidate
 // batch size n, and the n with the least predicted time for all nrhs,
 // ceil(nrhs / n) * t(n), wins.  Larger batches share each link load among
-// more right-hand sides but hold more registers and device memory.
+// more right-hand sides but hold more device memory.  Host-resident fields
+// take batches of at most 24, so that the transfers of one batch overlap the
+// solve of another; device-resident ones may advance as one set of up to 96.
+// A batch whose memory would exceed 45 % of the free device memory is not
+// tried.
 template <class SF, class XF, class LF>
-int tune_batch(cvcb_lattice *L, const cvcb_solver_params *P, int recon, int nrhs, int *nb_out) {
-  const int cands[] = {4, 6, 8, 12, 16, 24};
+int tune_batch(cvcb_lattice *L, const cvcb_solver_params *P, int recon, int nrhs, bool host_fields,
+               int *nb_out) {
+  const int cands[] = {4, 6, 8, 12, 16, 24, 32, 48, 96};
   double best_t = 1e300;
   int best = std::min(nrhs, 12);
+  size_t free_b = 0, total_b = 0;
+  CVCB_CUDA(cudaMemGetInfo(&free_b, &total_b));
   for (int n : cands) {
     if (n > kMaxBatch || (n > nrhs && n != cands[0])) continue;
+    if (host_fields && n > 24) continue;
+    const double need = 5.0 * 12 * L->g.V * sizeof(double2) * n +
+                        8.0 * sloppy_field_bytes<SF>(L->g.Vh, n);
+    if (n > cands[0] && need > 0.45 * (double)free_b) continue;
     Batch<SF, XF, LF> B;
     CVCB_TRY(setup_batch(L, B, n, /*with_fp64=*/false));
     CVCB_CUDA(cudaMemsetAsync(B.p.p, 0, sloppy_field_bytes<SF>(L->g.Vh, n), L->stream));
@@ -1549,26 +1621,32 @@ int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int
   int recon = P->link_recon;
   if (recon == 12 && !(L->unitarity >= 0 && L->unitarity < 1e-6)) recon = 18;  // not SU(3)
   std::memset(st, 0, sizeof *st);
+  bool host_fields = true;  // every field in host memory: batches pipeline the transfers
+  for (int i = 0; i < nrhs && host_fields; ++i)
+    host_fields = !is_device_ptr(x[i]) && !is_device_ptr(b[i]);
   int nb = P->block_rhs;
   if (!nb) {
     const bool pairs = P->precision == CVCB_PREC_SINGLE && use_pairs();
-    auto key = std::make_tuple(L->g.V, P->precision + (pairs ? kPairKey : 0), recon, nrhs);
+    auto key = std::make_tuple(L->g.V,
+                               P->precision + (pairs ? kPairKey : 0) + (host_fields ? 100 : 0),
+                               recon, nrhs);
     auto it = g_tuned_batch.find(key);
     if (it != g_tuned_batch.end()) {
       nb = it->second;
     } else {
       int rc;
+      const bool hf = host_fields;
       if (P->precision == CVCB_PREC_DOUBLE)
-        rc = tune_batch<F64Acc, F64Acc, L64>(L, P, recon, nrhs, &nb);
+        rc = tune_batch<F64Acc, F64Acc, L64>(L, P, recon, nrhs, hf, &nb);
       else if (pairs)
-        rc = recon == 12 ? tune_batch<P32, P32, LT32c>(L, P, recon, nrhs, &nb)
-                         : tune_batch<P32, P32, LT32f>(L, P, recon, nrhs, &nb);
+        rc = recon == 12 ? tune_batch<P32, P32, LT32c>(L, P, recon, nrhs, hf, &nb)
+                         : tune_batch<P32, P32, LT32f>(L, P, recon, nrhs, hf, &nb);
       else if (P->precision == CVCB_PREC_SINGLE)
-        rc = recon == 12 ? tune_batch<F32Acc, F32Acc, L32c>(L, P, recon, nrhs, &nb)
-                         : tune_batch<F32Acc, F32Acc, L32f>(L, P, recon, nrhs, &nb);
+        rc = recon == 12 ? tune_batch<F32Acc, F32Acc, L32c>(L, P, recon, nrhs, hf, &nb)
+                         : tune_batch<F32Acc, F32Acc, L32f>(L, P, recon, nrhs, hf, &nb);
       else
-        rc = recon == 12 ? tune_batch<F16Acc, F32Acc, L16c>(L, P, recon, nrhs, &nb)
-                         : tune_batch<F16Acc, F32Acc, L32f>(L, P, recon, nrhs, &nb);
+        rc = recon == 12 ? tune_batch<F16Acc, F32Acc, L16c>(L, P, recon, nrhs, hf, &nb)
+                         : tune_batch<F16Acc, F32Acc, L32f>(L, P, recon, nrhs, hf, &nb);
       if (rc < 0) return rc;
       g_tuned_batch[key] = nb;
     }
@@ -1586,9 +1664,7 @@ int solve_batched(cvcb_lattice *L, double *const *x, const double *const *b, int
     return recon == 12 ? run_batch<F16Acc, F32Acc, L16c>(L, xs, bs, n, P, st, nullptr, read)
                        : run_batch<F16Acc, F32Acc, L32f>(L, xs, bs, n, P, st, nullptr, read);
   };
-  bool host = nrhs > nb;
-  for (int i = 0; i < nrhs && host; ++i) host = !is_device_ptr(x[i]) && !is_device_ptr(b[i]);
-  if (host) {
+  if (host_fields && nrhs > nb) {
     const int rc = solve_pipelined(L, x, b, nrhs, nb, run);
     if (rc < 0) return rc;
   } else {
@@ -1654,6 +1730,15 @@ int cvcb_tuned_shape(cvcb_lattice *L, int precision, int link_recon, int nrhs, i
   *rhs_per_thread = s.nr;
   *variant = pairs ? 3 : s.pk ? 2 : (s.by > 1 && s.nr == 1) ? 1 : 0;
   return CVCB_OK;
+}
+
+int cvcb_sloppy_normal_op(cvcb_lattice *L, int precision, int link_recon, int layout, int nrhs,
+                          const double *const *in, double *const *out) {
+  if (!L || !in || !out) return CVCB_ERR_NULL;
+  for (int i = 0; i < nrhs; ++i)
+    if (!in[i] || !out[i]) return CVCB_ERR_NULL;
+  CVCB_CUDA(cudaSetDevice(L->device));
+  return cvcb::sloppy_normal_op(L, precision, link_recon, layout, nrhs, in, out);
 }
 
 int cvcb_time_stencil(cvcb_lattice *L, int kind, int precision, int link_recon, int nrhs,

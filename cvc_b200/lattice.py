@@ -193,6 +193,15 @@ class Lattice:
             raise CvcbError("invert_Qtm_her", rc)
         return (rc, float(tr[0])) if return_residual else rc
 
+    def sloppy_normal_op(self, ins, outs, precision, link_recon=12, layout=0):
+        """M^+ M of the batched solver's inner iterations on the odd sites of
+        CVC-layout fields (even sites of the outputs zero)."""
+        if len(ins) != len(outs):
+            raise ValueError("ins and outs differ in length")
+        _check("cvcb_sloppy_normal_op", self._lib.cvcb_sloppy_normal_op(
+            self._h, int(precision), int(link_recon), int(layout), len(ins), ptr_array(ins),
+            ptr_array(outs)))
+
     def solve(self, xs, bs, params=None):
         """Batched even/odd mixed-precision solve of Q x_i = b_i."""
         if params is None:

@@ -108,8 +108,34 @@ def p2gg(lat, source_site, dt, momentum, gamma_id, propagator_position=0, params
     return conn, contact, stats
 
 
+def source_positions(dims, n, seed):
+    """n source positions (lexicographic) from the ranlxd stream of `seed`,
+    4 numbers per position scaled to (T, LX, LY, LZ), as the benchmarks do."""
+    from . import lattice as _l
+    r = _l.ranlxd(4 * n, seed)
+    out = []
+    for k in range(n):
+        c = [int(r[4 * k + i] * m) % m for i, m in enumerate(dims)]
+        out.append(((c[0] * dims[1] + c[1]) * dims[2] + c[2]) * dims[3] + c[3])
+    return out
+
+
+def run_sources(sources, make_gauge, compute, n_gauge, device=None, group=None):
+    """The multi-source P -> gamma gamma run on one or several ranks (one
+    process per GPU): rank 0 makes the gauge field and broadcasts it (one
+    collective, before any solve), every rank takes its round-robin share of
+    the source positions, and Pi of all sources is gathered on every rank.
+    compute(gauge, source) -> (conn, contact) tensors on `device`; returns
+    (conn [n_sources, 32 V], contact [n_sources, 8])."""
+    from . import sharding
+    world, rank = sharding.world_rank(group)
+    gauge = sharding.broadcast_field(make_gauge() if rank == 0 else None, n_gauge, device, group)
+    return sharding.pi_sharded(sources, lambda s: compute(gauge, s), group)
+
+
 def main(argv=None):
-    ap = argparse.ArgumentParser(description="P -> gamma gamma pipeline on one GPU")
+    ap = argparse.ArgumentParser(description="P -> gamma gamma pipeline, one process per GPU "
+                                             "(under torchrun for several GPUs)")
     ap.add_argument("--dims", type=int, nargs=4, default=(64, 32, 32, 32),
                     metavar=("T", "LX", "LY", "LZ"))
     ap.add_argument("--kappa", type=float, default=0.156)
@@ -121,32 +147,53 @@ def main(argv=None):
     ap.add_argument("--precision", default="single", choices=("double", "single", "half"))
     ap.add_argument("--block-rhs", type=int, default=12)
     a = ap.parse_args(argv)
+    import os
     import torch
-    from . import lattice as _l
+    import torch.distributed as dist
+    from . import sharding
     dims = tuple(a.dims)
     V = int(np.prod(dims))
-    lat = Lattice(*dims, kappa=a.kappa, mu=a.mu2k / (2 * a.kappa),
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=device)
+    lat = Lattice(*dims, device=local, kappa=a.kappa, mu=a.mu2k / (2 * a.kappa),
                   bc_angle=(1.0, 0.0, 0.0, 0.0))
-    lat.upload_gauge(gauge_random(*dims, a.eps, a.seed))
     p = solver_defaults()
     p.precision = {"double": 0, "single": 1, "half": 2}[a.precision]
     p.link_recon = 18 if p.precision == 0 else 12
     p.block_rhs = a.block_rhs
-    # source positions: ranlxd stream of the seed, as the solver benchmark does
-    r = _l.ranlxd(4 * a.sources, a.seed)
+    sources = source_positions(dims, a.sources, a.seed)
     tot = {"solves": 0, "solve_s": 0.0, "contract_s": 0.0}
-    for k in range(a.sources):
-        c = [int(r[4 * k + i] * n) % n for i, n in enumerate(dims)]
-        site = ((c[0] * dims[1] + c[1]) * dims[2] + c[2]) * dims[3] + c[3]
-        conn, contact, st = p2gg(lat, site, a.dt, (0, 0, 0), 5, 0, p)
+    uploaded = []
+
+    def compute(gauge, site):
+        if not uploaded:
+            lat.upload_gauge(gauge)
+            uploaded.append(True)
+        conn, contact, st = p2gg(lat, site, a.dt, (0, 0, 0), 5, 0, p, device=device)
         for key in tot:
             tot[key] += st[key]
-        print(f"source {c}: {st['solves']} solves in {st['solve_s']:.2f} s "
-              f"(max true residual {st['max_true_res']:.2e}), contraction {st['contract_s']:.3f} s, "
-              f"|Pi| = {float(torch.linalg.norm(conn)):.6e}")
-    print(f"total: {tot['solves']} solves, {tot['solves'] / tot['solve_s']:.1f} solves/s, "
-          f"contraction {tot['contract_s'] / a.sources:.3f} s per source, V = {V}")
+        print(f"[rank {sharding.world_rank()[1]}] source {site}: {st['solves']} solves in "
+              f"{st['solve_s']:.2f} s (max true residual {st['max_true_res']:.2e}), contraction "
+              f"{st['contract_s']:.3f} s", flush=True)
+        return conn, torch.as_tensor(contact, device=device)
+
+    conn, contact = run_sources(sources, lambda: gauge_random(*dims, a.eps, a.seed), compute,
+                                72 * V, device)
+    solve_s = sharding.max_over_ranks(tot["solve_s"], device)
+    if sharding.world_rank()[1] == 0:
+        for k, s in enumerate(sources):
+            print(f"source {s}: |Pi| = {float(torch.linalg.norm(conn[k])):.6e}")
+        n = 180 * len(sources)
+        print(f"total: {n} solves on {world} GPU(s), {n / solve_s:.1f} solves/s (slowest rank), "
+              f"V = {V}")
     lat.close()
+    if world > 1:
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -58,6 +58,40 @@ def gather_tensors(local, n_items, group=None):
     return torch.stack(rows)
 
 
+def broadcast_field(field, n, device=None, group=None, src=0):
+    """Rank `src` holds `field` (n doubles, numpy or None elsewhere); every
+    rank returns it as a numpy array after one broadcast (over NVLink with
+    NCCL when `device` is a CUDA device).  The gauge field is generated once
+    and sent, instead of being generated on every rank."""
+    import numpy as np
+    world, rank = world_rank(group)
+    if world == 1:
+        return np.ascontiguousarray(field, np.float64)
+    if rank == src:
+        t = torch.from_numpy(np.ascontiguousarray(field, np.float64)).to(device or "cpu")
+    else:
+        t = torch.empty(n, dtype=torch.float64, device=device or "cpu")
+    dist.broadcast(t, src, group=group)
+    return t.cpu().numpy()
+
+
+def pi_sharded(sources, compute, group=None):
+    """Pi_mu_nu for every source position, computed by the rank that owns it
+    (round-robin) and gathered: compute(source) -> (conn tensor of 32*V
+    doubles, contact tensor of 8 doubles) on this rank's device; returns
+    (conn [n_sources, 32*V], contact [n_sources, 8]) on every rank."""
+    world, rank = world_rank(group)
+    if len(sources) < world:  # the same decision on every rank, before any collective
+        raise ValueError(f"{len(sources)} source positions for {world} ranks")
+    mine = my_items(range(len(sources)), world, rank)
+    conns, contacts = [], []
+    for i in mine:
+        c, ct = compute(sources[i])
+        conns.append(c)
+        contacts.append(ct)
+    return gather_tensors(conns, len(sources), group), gather_tensors(contacts, len(sources), group)
+
+
 def max_over_ranks(value, device=None, group=None):
     """Maximum of a float over ranks (step times are reported this way)."""
     world, _ = world_rank(group)

@@ -211,7 +211,9 @@ int cvcb_invert_Qtm_her(cvcb_lattice *lat, double *xi, const double *phi,
 typedef struct {
   int precision;     /* CVCB_PREC_*: arithmetic/storage of the inner iterations */
   int link_recon;    /* 18 or 12 reals per link in the inner operator */
-  int block_rhs;     /* right-hand sides per launch (0 = autotuned) */
+  int block_rhs;     /* right-hand sides per batch, at most 96 (0 = autotuned:
+                        up to 96 for device fields, up to 24 for host fields,
+                        whose transfers overlap the solve of another batch) */
   int block_threads; /* sites per stencil block, one rhs per thread; a multiple
                         of 32 up to 256 (0 = autotuned shape) */
   int max_iter;      /* per right-hand side */
@@ -254,12 +256,26 @@ int cvcb_solve(cvcb_lattice *lat, double *const *x, const double *const *b, int 
 int cvcb_time_stencil(cvcb_lattice *lat, int kind, int precision, int link_recon, int nrhs,
                       int reps, double *ms_per_launch);
 
+/* The normal operator M^+ M of the batched solver's inner iterations, as
+ * the solver applies it: in[i] -> out[i] for i < nrhs (nrhs <= 96), CVC-layout
+ * FP64 fields (host or device); the odd sites of in are the input (M is the
+ * odd-site Schur complement A_oo - 1/4 H_oe A_ee^-1 H_eo of Q_phi_tbc's
+ * operator, M(mu)^+ = g5 M(-mu) g5), even sites of out are set to zero.  The
+ * fields go through the storage of `precision` (CVCB_PREC_*) with
+ * link_recon reals per link; layout 1 selects the pair-tiled FP32 storage
+ * (precision CVCB_PREC_SINGLE only), layout 0 the per-rhs one.  For checking
+ * the reduced-precision operators against the FP64 one.  No counterpart in
+ * the reference. */
+int cvcb_sloppy_normal_op(cvcb_lattice *lat, int precision, int link_recon, int layout, int nrhs,
+                          const double *const *in, double *const *out);
+
 /* Launch shape the autotuner chose for the batched stencil for this lattice
  * volume, precision, link format and batch size: sites per thread block,
  * thread rows per block (each row a group of right-hand sides), right-hand
  * sides per thread, and the kernel variant (0: links per thread, 1: links
  * staged in shared memory for all rows, 2: two rhs per thread in packed
- * FP32x2 arithmetic); CVCB_ERR_STATE before the first tuning. */
+ * FP32x2 arithmetic, 3: pair-tiled fields); CVCB_ERR_STATE before the first
+ * tuning. */
 int cvcb_tuned_shape(cvcb_lattice *lat, int precision, int link_recon, int nrhs,
                      int *sites_per_block, int *rows_per_block, int *rhs_per_thread,
                      int *variant);

@@ -61,6 +61,7 @@ def test_stencil_variants_agree(prec):
     if prec == 1:
         res.update({f"pairs {v} {r}": run(prec, v, pt, r) for v, pt, r in PAIR_VARIANTS})
     base = res["64,1,1"]
+    print({v: r["iters"] for v, r in res.items()})
     for v, r in res.items():
         assert r["conv"] == 11, (v, r)
         assert r["res"] <= 1e-10 and r["chk"] <= 1e-10, (v, r)
