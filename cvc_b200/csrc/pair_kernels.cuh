@@ -21,7 +21,6 @@
 #pragma once
 
 #include "eo_kernels.cuh"
-#include "reduce.cuh"
 
 namespace cvcb {
 
@@ -188,14 +187,18 @@ __device__ __forceinline__ void diag_pair(SpinorPair &o, const SpinorPair &v, co
     }
 }
 
-__device__ __forceinline__ float2 norm2_pair(const SpinorPair &v) {
-  float2 n = make_float2(0.f, 0.f);
+// |v|^2 of one site for both right-hand sides, accumulated in FP64
+__device__ __forceinline__ double2 norm2_pair(const SpinorPair &v) {
+  double2 n = make_double2(0.0, 0.0);
 #pragma unroll
   for (int s = 0; s < 4; ++s)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      n = __ffma2_rn(v.c[s][c].re, v.c[s][c].re, n);
-      n = __ffma2_rn(v.c[s][c].im, v.c[s][c].im, n);
+      const CP &z = v.c[s][c];
+      n.x = fma((double)z.re.x, (double)z.re.x, n.x);
+      n.x = fma((double)z.im.x, (double)z.im.x, n.x);
+      n.y = fma((double)z.re.y, (double)z.re.y, n.y);
+      n.y = fma((double)z.im.y, (double)z.im.y, n.y);
     }
   return n;
 }
@@ -263,7 +266,7 @@ __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_pt(HopArgs<P32, LF
   }
   for (int sb = blockIdx.y; sb * (int)blockDim.x < g.Vh; sb += gridDim.y) {
     const int i = sb * blockDim.x + threadIdx.x;
-    float2 n2 = make_float2(0.f, 0.f);  // |out|^2 of this site, rhs a and b
+    double2 n2 = make_double2(0.0, 0.0);  // |out|^2 (or |r|^2) of this site, rhs a and b
     if (i < g.Vh) {
       const SiteCoord cd = site_coord(g, p, i);
       const int self = p * g.Vh + i;
@@ -309,53 +312,6 @@ __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_pt(HopArgs<P32, LF
         if (has_b) A.dot_part[(size_t)(ra + 1) * A.dot_np + w] = db;
       }
     }
-  }
-}
-
-// ---- pair reductions: blockIdx.y = pair, both right-hand sides at once -----
-// F: __device__ double2 operator()(int pr, int s, bool act_a, bool act_b)
-// E: __device__ void operator()(int r, double total)
-// skip[r] != 0 leaves rhs r out (its lane is neither updated nor reported).
-template <class F, class E>
-__global__ void __launch_bounds__(kRedThreads)
-    k_reduce_pair(F f, E e, int nsites, int nrhs, double *partials, unsigned *counters,
-                  const int *__restrict__ skip) {
-  const int pr = blockIdx.y;
-  const int ra = 2 * pr;
-  const bool has_b = ra + 1 < nrhs;
-  const bool act_a = !(skip && skip[ra]);
-  const bool act_b = has_b && !(skip && skip[ra + 1]);
-  if (!act_a && !act_b) return;
-  __shared__ double sh[2][kRedThreads / 32];
-  __shared__ bool last;
-  double v[2] = {0.0, 0.0};
-  for (int s = blockIdx.x * kRedThreads + threadIdx.x; s < nsites; s += gridDim.x * kRedThreads) {
-    const double2 t = f(pr, s, act_a, act_b);
-    v[0] += t.x;
-    v[1] += t.y;
-  }
-  block_sum<2>(v, sh);
-  double *pa = partials + (size_t)ra * kMaxRedBlocks;
-  double *pb = pa + kMaxRedBlocks;
-  if (threadIdx.x == 0) {
-    pa[blockIdx.x] = v[0];
-    if (has_b) pb[blockIdx.x] = v[1];
-    __threadfence();
-    last = atomicAdd(counters + pr, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  v[0] = v[1] = 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += kRedThreads) {
-    v[0] += __ldcg(pa + b);
-    if (has_b) v[1] += __ldcg(pb + b);
-  }
-  block_sum<2>(v, sh);
-  if (threadIdx.x == 0) {
-    counters[pr] = 0;
-    if (act_a) e(ra, v[0]);
-    if (act_b) e(ra + 1, v[1]);
   }
 }
 

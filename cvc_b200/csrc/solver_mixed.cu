@@ -985,8 +985,9 @@ int time_ms(cvcb_lattice *L, Fn fn, int reps, float *best) {
 // per block, timed on the sloppy normal operator.
 template <class SF, class XF, class LF>
 int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int block_threads = 0) {
-  if (block_threads > 0) {  // caller's choice: that many sites per block, one rhs per thread
-    B.shape = LaunchShape{block_threads, 1, 1};
+  if (block_threads > 0) {  // caller's choice: that many sites per block, one rhs (pair) per thread
+    B.shape = std::is_same<SF, P32>::value ? LaunchShape{block_threads, 1, 2, 1}
+                                           : LaunchShape{block_threads, 1, 1};
     return CVCB_OK;
   }
   constexpr bool pairs = std::is_same<SF, P32>::value;
@@ -1202,7 +1203,7 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   // drifts from the true residual after about three decades, FP32 after six
   const double delta = P->delta > 0 ? P->delta
                        : std::is_same<SF, F16Acc>::value ? 0.1
-                       : std::is_same<SF, F32Acc>::value ? 1e-4 : 1e-8;
+                       : sizeof(typename SF::R) == 4 ? 1e-4 : 1e-8;
   const double delta2 = delta * delta;
   int total_iter = 0, nru = 0, nrestart = 0;
   // rr at the previous check (same units) and the measured per-iteration
@@ -1434,11 +1435,12 @@ int sloppy_normal_op(cvcb_lattice *L, int prec, int recon, int layout, int n,
 }
 
 // FP32 inner iterations on pair-tiled fields (k_eo_hop_pt and the pair CG
-// kernels) instead of per-rhs fields: CVCB_PAIRS=1 (read once).
+// kernels), the default; CVCB_PAIRS=0 selects the per-rhs fields with the
+// packed-pair stencil k_eo_hop_x2 instead (read once per process).
 bool use_pairs() {
   static const bool on = [] {
     const char *e = getenv("CVCB_PAIRS");
-    return e && atoi(e) != 0;
+    return !e || atoi(e) != 0;
   }();
   return on;
 }

@@ -214,7 +214,8 @@ typedef struct {
   int block_rhs;     /* right-hand sides per batch, at most 96 (0 = autotuned:
                         up to 96 for device fields, up to 24 for host fields,
                         whose transfers overlap the solve of another batch) */
-  int block_threads; /* sites per stencil block, one rhs per thread; a multiple
+  int block_threads; /* sites per stencil block, one rhs (FP32: one rhs pair) per
+                        thread; a multiple
                         of 32 up to 256 (0 = autotuned shape) */
   int max_iter;      /* per right-hand side */
   int use_graph;     /* capture the inner iterations in a CUDA graph */
