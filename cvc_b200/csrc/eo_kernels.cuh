@@ -273,6 +273,8 @@ struct HopArgs {
   // |r|^2)
   SF rup;
   const double *alpha;
+  // k_eo_hop_ptb: set to 1 if a staged copy did not complete in time
+  int *err;
 };
 
 // |a|^2 of one site, accumulated in FP64

@@ -315,4 +315,221 @@ __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_pt(HopArgs<P32, LF
   }
 }
 
+// ---- the same sweep with the t and x neighbours staged by bulk copies -------
+// On lattices with LY*LZ/2 a multiple of 32, the 32 sites of a tile share
+// their t and x coordinates, so the t+-, x+- neighbours of a tile are again
+// one whole tile (6 KB per rhs pair): one cp.async.bulk each, issued by lane 0
+// of the warp that owns the tile into shared memory and completed on an
+// mbarrier.  The two t copies start before the z and y hops (plain loads,
+// mostly L1 hits) are computed, the x copies reuse the stage buffers as soon
+// as the t data has been read, so the long-latency neighbours arrive while
+// the warp computes and hold no registers while in flight.  Waits are
+// bounded: a copy not complete after about a second sets *err and the
+// kernel returns after a bounded wait for the copies it still has in flight.
+constexpr int kBulkWarps = 4;  // warps per block: 4 consecutive tiles of one rhs pair
+constexpr unsigned kTileBytes = 12 * kTile * sizeof(float4);  // 6144
+constexpr size_t kBulkSmem = (size_t)kBulkWarps * 2 * kTileBytes;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// one arrival that also announces `bytes` of transaction for this phase
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                         unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the phase with the given parity to complete
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+  for (int n = 0; n < (1 << 20); ++n)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ SpinorPair stage_load(const float4 *S, int lane) {
+  SpinorPair f;
+#pragma unroll
+  for (int k = 0; k < 12; ++k) f.c[k / 3][k % 3] = cp_of(S[k * kTile + lane]);
+  return f;
+}
+
+template <int MU, int S>
+__device__ __forceinline__ void hop_from(SpinorPair &acc, const Link<float> &W,
+                                         const SpinorPair &f, bool g5in) {
+  if (S > 0) {  // backward: (1 + g_mu) U_mu(x-mu)^+ in(x-mu)
+    const HalfPair h = g5in ? project_pair<MU, -1>(f) : project_pair<MU, +1>(f);
+    accum_recon_pair(MU, +1, acc, link_mul_pair<true>(W, h));
+  } else {  // forward: (1 - g_mu) U_mu(x) in(x+mu)
+    const HalfPair h = g5in ? project_pair<MU, +1>(f) : project_pair<MU, -1>(f);
+    accum_recon_pair(MU, -1, acc, link_mul_pair<false>(W, h));
+  }
+}
+
+// Block = kBulkWarps warps on consecutive tiles of rhs pair blockIdx.x;
+// dynamic shared memory kBulkSmem.  dot_part (if given) holds one partial
+// per tile (dot_np = V/2 / 32).
+template <class LF, bool G5IN, bool G5HOP, bool AUX, bool RUPD = false>
+__global__ void __launch_bounds__(kBulkWarps * 32, 4) k_eo_hop_ptb(HopArgs<P32, LF> A) {
+  extern __shared__ __align__(128) float4 stage[];
+  __shared__ __align__(8) unsigned long long bars[kBulkWarps][2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pr = blockIdx.x;
+  const int ra = 2 * pr;
+  if (ra >= A.nrhs) return;  // uniform over the block
+  const bool act_a = !(A.done && A.done[ra]);
+  const bool has_b = ra + 1 < A.nrhs;
+  const bool act_b = has_b && !(A.done && A.done[ra + 1]);
+  if (!act_a && !act_b) return;  // uniform over the block
+  const Geom &g = A.eg.g;
+  const int p = A.eg.p;
+  const int qoff = (1 - p) * g.Vh;
+  float a1[4], b1[4], a2[4], b2[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const float g5 = s < 2 ? 1.f : -1.f;
+    const float gh = G5HOP ? g5 : 1.f;
+    a1[s] = (float)(A.c * A.d1a) * gh;
+    b1[s] = (float)(A.c * A.d1b) * g5 * gh;
+    a2[s] = (float)A.d2a;
+    b2[s] = (float)A.d2b * g5;
+  }
+  float4 *S0 = stage + (size_t)warp * 2 * 12 * kTile, *S1 = S0 + 12 * kTile;
+  unsigned long long *b0 = &bars[warp][0], *b1b = &bars[warp][1];
+  if (lane == 0) {
+    mbar_init(b0, 1);
+    mbar_init(b1b, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  unsigned ph0 = 0, ph1 = 0;
+  const int ntiles = g.Vh / kTile;
+  const float4 *in_pair = A.in.p + (size_t)pr * A.in.pstride;
+  for (int tile = blockIdx.y * kBulkWarps + warp; tile < ntiles;
+       tile += gridDim.y * kBulkWarps) {
+    const int i = tile * kTile + lane;
+    const SiteCoord cd = site_coord(g, p, i);
+    const int self = p * g.Vh + i;
+    const int jtm = nb_lex(g, cd, 0, -1) >> 1, jtp = nb_lex(g, cd, 0, +1) >> 1;
+    const int jxm = nb_lex(g, cd, 1, -1) >> 1, jxp = nb_lex(g, cd, 1, +1) >> 1;
+    if (lane == 0) {  // whole neighbour tiles: lane 0's neighbour is the tile start
+      fence_proxy_async();  // the previous tile's reads of S0, S1 come first
+      mbar_expect_tx(b0, kTileBytes);
+      bulk_g2s(S0, in_pair + (size_t)(jtm >> 5) * 12 * kTile, kTileBytes, b0);
+      mbar_expect_tx(b1b, kTileBytes);
+      bulk_g2s(S1, in_pair + (size_t)(jtp >> 5) * 12 * kTile, kTileBytes, b1b);
+    }
+    SpinorPair acc;
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc.c[s][c].re = acc.c[s][c].im = make_float2(0.f, 0.f);
+    hop_pair_dir<3>(acc, A, cd, pr, self, qoff, G5IN);
+    hop_pair_dir<2>(acc, A, cd, pr, self, qoff, G5IN);
+    // every wait's outcome is made warp-uniform, so all lanes take the same
+    // branches (and reach every __syncwarp)
+    bool ok = __all_sync(0xffffffffu, mbar_wait(b0, ph0));
+    if (ok) {
+      ph0 ^= 1;
+      hop_from<0, +1>(acc, A.links.load(0, qoff + jtm), stage_load(S0, lane), G5IN);
+      __syncwarp();
+      if (lane == 0) {
+        fence_proxy_async();
+        mbar_expect_tx(b0, kTileBytes);
+        bulk_g2s(S0, in_pair + (size_t)(jxm >> 5) * 12 * kTile, kTileBytes, b0);
+      }
+      ok = __all_sync(0xffffffffu, mbar_wait(b1b, ph1));
+    }
+    if (ok) {
+      ph1 ^= 1;
+      hop_from<0, -1>(acc, A.links.load(0, self), stage_load(S1, lane), G5IN);
+      __syncwarp();
+      if (lane == 0) {
+        fence_proxy_async();
+        mbar_expect_tx(b1b, kTileBytes);
+        bulk_g2s(S1, in_pair + (size_t)(jxp >> 5) * 12 * kTile, kTileBytes, b1b);
+      }
+      ok = __all_sync(0xffffffffu, mbar_wait(b0, ph0));
+    }
+    if (ok) {
+      ph0 ^= 1;
+      hop_from<1, +1>(acc, A.links.load(1, qoff + jxm), stage_load(S0, lane), G5IN);
+      ok = __all_sync(0xffffffffu, mbar_wait(b1b, ph1));
+    }
+    if (!ok) {
+      // a copy did not complete: report, let the copies in flight land
+      // (bounded), leave
+      if (lane == 0 && A.err) atomicExch(A.err, 1);
+      mbar_wait(b0, ph0);
+      mbar_wait(b1b, ph1);
+      return;
+    }
+    ph1 ^= 1;
+    hop_from<1, -1>(acc, A.links.load(1, self), stage_load(S1, lane), G5IN);
+    __syncwarp();
+    SpinorPair o;
+    diag_pair(o, acc, a1, b1, false);
+    if (AUX) diag_pair(o, A.aux.load_pair(pr, i), a2, b2, true);
+    double2 n2 = make_double2(0.0, 0.0);
+    if (RUPD) {
+      const float2 na = make_float2(-(float)A.alpha[ra], has_b ? -(float)A.alpha[ra + 1] : 0.f);
+      SpinorPair rv = A.rup.load_pair(pr, i);
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          rv.c[s][c].re = __ffma2_rn(na, o.c[s][c].re, rv.c[s][c].re);
+          rv.c[s][c].im = __ffma2_rn(na, o.c[s][c].im, rv.c[s][c].im);
+        }
+      if (A.dot_part) n2 = norm2_pair(rv);
+      store_active(A.rup, pr, i, rv, act_a, act_b);
+    } else {
+      if (A.dot_part) n2 = norm2_pair(o);
+      store_active(A.out, pr, i, o, act_a, act_b);
+    }
+    if (A.dot_part) {
+      double da = n2.x, db = n2.y;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        da += __shfl_down_sync(0xffffffffu, da, o);
+        db += __shfl_down_sync(0xffffffffu, db, o);
+      }
+      if (lane == 0) {
+        A.dot_part[(size_t)ra * A.dot_np + tile] = da;
+        if (has_b) A.dot_part[(size_t)(ra + 1) * A.dot_np + tile] = db;
+      }
+    }
+  }
+}
+
+// Whether a lattice admits k_eo_hop_ptb: the t and x neighbours of a tile
+// are whole tiles when LY*LZ/2 is a multiple of 32.
+inline bool bulk_stencil_ok(const Geom &g) { return (g.LY * g.LZ / 2) % kTile == 0; }
+
 }  // namespace cvcb

@@ -535,6 +535,7 @@ struct Batch {
   // that produces M p
   double *dot_part = nullptr;
   int dot_np = 0;
+  int *err = nullptr;  // set by a stencil whose staged copy did not complete
   int *ru_skip;   // per rhs: 1 = skip in the reliable update
   int *rst_skip;  // per rhs: 0 = restart the direction from the residual
   BatchRed br;
@@ -568,9 +569,10 @@ struct Batch {
         return CVCB_ERR_STATE;
       }
       a.dot_part = dot_part;
-      a.dot_np = ((g.Vh + shape.bx - 1) / shape.bx) * (shape.bx / 32);
+      a.dot_np = dot_parts();
       dot_np = a.dot_np;
     }
+    a.err = err;
     // FP64 sweeps of a reduced-precision solve (reliable updates) have their
     // own tuned shape; FP64 kernels keep one rhs per thread (register budget).
     LaunchShape sh = sizeof(typename AF::R) == 8 && sizeof(typename SF::R) != 8 ? shape64 : shape;
@@ -588,7 +590,7 @@ struct Batch {
     }
     bool packed = false;
     if constexpr (std::is_same<AF, P32>::value) {  // pair-tiled fields
-      k_eo_hop_pt<LL, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a);
+      CVCB_TRY((launch_pt<LL, G5IN, G5HOP, AUX, false>(a, sh)));
       packed = true;
     } else if constexpr (sizeof(typename AF::R) == 4) {
       if (sh.pk) {  // two rhs per thread in packed FP32x2 arithmetic
@@ -629,7 +631,7 @@ struct Batch {
         default: k_eo_hop<AF, LL, 1, G5IN, G5HOP, AUX><<<grid, block, 0, L->stream>>>(a); break;
       }
     }
-    CVCB_LAUNCHED(L);
+    if (!std::is_same<AF, P32>::value) CVCB_LAUNCHED(L);  // launch_pt counts its own
     if (rec_this) {
       CVCB_CUDA(cudaEventRecordWithFlags(rec.b, L->stream, capturing ? cudaEventRecordExternal : 0));
       rec.bytes_per_rhs = (double)g.Vh * spinor_bytes<AF>() * (AUX ? 3 : 2);
@@ -650,22 +652,18 @@ struct Batch {
         return CVCB_ERR_STATE;
       }
       a.dot_part = dot_part;
-      a.dot_np = ((g.Vh + shape.bx - 1) / shape.bx) * (shape.bx / 32);
+      a.dot_np = dot_parts();
       dot_np = a.dot_np;
       a.rup = rs;
       a.alpha = S.alpha;
-      const int groups = (n + 1) / 2;
-      const int by = std::min(shape.by, groups);
-      const int site_blocks = (g.Vh + shape.bx - 1) / shape.bx;
-      dim3 block(shape.bx, by), grid((groups + by - 1) / by, std::min(site_blocks, 65535));
+      a.err = err;
       Rec rec{};
       if (prof_rec) {
         CVCB_CUDA(cudaEventCreate(&rec.a));
         CVCB_CUDA(cudaEventCreate(&rec.b));
         CVCB_CUDA(cudaEventRecordWithFlags(rec.a, L->stream, capturing ? cudaEventRecordExternal : 0));
       }
-      k_eo_hop_pt<LF, false, true, true, true><<<grid, block, 0, L->stream>>>(a);
-      CVCB_LAUNCHED(L);
+      CVCB_TRY((launch_pt<LF, false, true, true, true>(a, shape)));
       if (prof_rec) {
         CVCB_CUDA(cudaEventRecordWithFlags(rec.b, L->stream, capturing ? cudaEventRecordExternal : 0));
         // neighbours, aux, r read and r written
@@ -690,9 +688,46 @@ struct Batch {
   }
 
   // <p, M^+M p> = |M p|^2 in the sweep that writes M p: the packed FP32x2
-  // kernel with blocks a multiple of a warp wide
+  // kernels with blocks a multiple of a warp wide
   bool dot_fusable() const {
-    return sizeof(typename SF::R) == 4 && shape.pk == 1 && shape.bx % 32 == 0;
+    return sizeof(typename SF::R) == 4 && shape.pk >= 1 && shape.bx % 32 == 0;
+  }
+  // partial sums per rhs of the fused norms: one per warp of the site blocks
+  // (one per 32-site tile for the bulk-staged stencil)
+  int dot_parts() const {
+    if (shape.pk == 2) return g.Vh / kTile;
+    return ((g.Vh + shape.bx - 1) / shape.bx) * (shape.bx / 32);
+  }
+
+  // Pair-tiled stencil launch: pk 2 = bulk-staged t and x neighbours
+  // (k_eo_hop_ptb, whole-tile lattices only), else plain loads (k_eo_hop_pt)
+  template <class LL, bool G5IN, bool G5HOP, bool AUX, bool RUPD>
+  int launch_pt(const HopArgs<P32, LL> &a, const LaunchShape &sh) {
+    const int groups = (n + 1) / 2;
+    if (sh.pk == 2) {
+      if (!bulk_stencil_ok(g) || !a.err) {
+        set_error("bulk-staged stencil needs LY*LZ/2 a multiple of 32");
+        return CVCB_ERR_ARG;
+      }
+      auto kern = k_eo_hop_ptb<LL, G5IN, G5HOP, AUX, RUPD>;
+      static std::atomic<unsigned long long> attr_set{0};  // per instantiation, bit per device
+      const unsigned long long bit = 1ull << (L->device & 63);
+      if (!(attr_set.load() & bit)) {
+        CVCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kBulkSmem));
+        attr_set.fetch_or(bit);
+      }
+      const int tiles = g.Vh / kTile;
+      dim3 grid(groups, std::min((tiles + kBulkWarps - 1) / kBulkWarps, 65535));
+      kern<<<grid, kBulkWarps * 32, kBulkSmem, L->stream>>>(a);
+    } else {
+      const int by = std::min(sh.by, groups);
+      const int site_blocks = (g.Vh + sh.bx - 1) / sh.bx;
+      dim3 block(sh.bx, by), grid((groups + by - 1) / by, std::min(site_blocks, 65535));
+      k_eo_hop_pt<LL, G5IN, G5HOP, AUX, RUPD><<<grid, block, 0, L->stream>>>(a);
+    }
+    CVCB_LAUNCHED(L);
+    return CVCB_OK;
   }
 
   // out_o = M^+ M in_o with sloppy fields (te, yo, te2 as intermediates);
@@ -908,7 +943,7 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
                       rnd(sizeof(unsigned) * kMaxBatch);
   const size_t dotb = sizeof(double) * (size_t)n * (g.Vh / 32 + 64);
   const size_t total = 5 * rnd(f64) + 6 * (rnd(sl) + rnd(nrm)) + rnd(xsl) + rnd(nrm) + scal + part +
-                       rnd(dotb);
+                       rnd(dotb) + rnd(sizeof(int));
   void *mem;
   CVCB_TRY(ensure_buffer(L, SLOT_MIX0, total, &mem));
   char *p = static_cast<char *>(mem);
@@ -949,6 +984,8 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   B.br.partials = (double *)take(sizeof(double) * kMaxRedBlocks * kMaxBatch);
   B.br.counters = (unsigned *)take(sizeof(unsigned) * kMaxBatch);
   B.dot_part = (double *)take(dotb);
+  B.err = (int *)take(sizeof(int));
+  CVCB_CUDA(cudaMemsetAsync(B.err, 0, sizeof(int), L->stream));
   CVCB_CUDA(cudaMemsetAsync(B.br.counters, 0, sizeof(unsigned) * kMaxBatch, L->stream));
   CVCB_CUDA(cudaMemsetAsync(B.S.done, 0, sizeof(int) * kMaxBatch, L->stream));
   CVCB_CUDA(cudaMemsetAsync(B.ru_skip, 0, sizeof(int) * kMaxBatch, L->stream));
@@ -1006,13 +1043,19 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
         f.bx * f.by <= kHopMaxThreads) {
       if (nf < 4 || f.nr != 2) f.pk = 0;
       if (sizeof(typename SF::R) == 8) f.nr = 1, f.pk = 0;
-      if (pairs) f.nr = 2, f.pk = 1;  // pair-tiled fields: one rhs pair per thread
+      if (pairs) {  // pair-tiled fields: one rhs pair per thread; 4th field 2 = bulk-staged
+        f.nr = 2;
+        f.pk = (nf >= 4 && f.pk == 2 && bulk_stencil_ok(L->g)) ? 2 : 1;
+        if (f.pk == 2) f.bx = kBulkWarps * 32, f.by = 1;
+      }
       B.shape = f;
       g_tuned_shape[key] = f;
       return CVCB_OK;
     }
   }
-  LaunchShape best;
+  // a pair-tiled batch always has a valid shape: one pair per thread, even
+  // for a single right-hand side (the second lane of its pair idles)
+  LaunchShape best = pairs ? LaunchShape{64, 1, 2, 1} : LaunchShape{};
   float best_ms = 1e30f;
   const int bxs[] = {32, 64, 128, 256};
   const int bys[] = {1, 2, 3, 4, 6};
@@ -1026,7 +1069,8 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
       const int nr = np[0];
       if (fp64 && nr > 1) continue;
       if (pairs && !(nr == 2 && np[1] == 1)) continue;
-      if (nr > B.n || by * nr > B.n || bx * by > kHopMaxThreads || bx * by < 32) continue;
+      if (bx * by > kHopMaxThreads || bx * by < 32) continue;
+      if (pairs ? by > (B.n + 1) / 2 : (nr > B.n || by * nr > B.n)) continue;
       B.shape.bx = bx;
       B.shape.by = by;
       B.shape.nr = nr;
@@ -1041,6 +1085,16 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
         best = B.shape;
       }
     }
+  if (pairs && bulk_stencil_ok(L->g)) {  // the bulk-staged stencil: one fixed block shape
+    B.shape = LaunchShape{kBulkWarps * 32, 1, 2, 2};
+    float ms;
+    if (time_ms(L, [&] { return B.normal_op_sloppy(B.Ap, B.p, nullptr); }, 3, &ms) != CVCB_OK) {
+      cudaGetLastError();
+    } else if (ms < best_ms) {
+      best_ms = ms;
+      best = B.shape;
+    }
+  }
   B.shape = best;
   g_tuned_shape[key] = best;
   return CVCB_OK;
@@ -1339,6 +1393,13 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     const double rel = hb2[i] > 0 ? std::sqrt(rhat2[i] / hb2[i]) : 0.0;
     worst = std::max(worst, rel);
     if (rel <= P->tol) ++nconv;
+  }
+  int staged_err = 0;
+  CVCB_CUDA(cudaMemcpyAsync(&staged_err, B.err, sizeof(int), cudaMemcpyDeviceToHost, L->stream));
+  CVCB_CUDA(cudaStreamSynchronize(L->stream));
+  if (staged_err) {
+    set_error("a staged neighbour copy of the stencil did not complete in time");
+    return CVCB_ERR_CUDA;
   }
   st->iterations += std::accumulate(iters.begin(), iters.end(), 0);
   st->reliable_updates += nru;
