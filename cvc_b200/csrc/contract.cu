@@ -81,7 +81,11 @@ __device__ __forceinline__ Spinor<double> recon_full(int mu, int s, const HalfSp
 // Pi_mu_nu for one nu: P0 = up columns of part 0 (unshifted source),
 // P1 = up columns of part 1 (source shifted by nu), Z = 24 columns from
 // k_cvc_z.  conn is CVC layout (lexicographic, 32 doubles per site).
-__global__ void __launch_bounds__(128) k_cvc_pi(double *__restrict__ conn,
+// MINB: minimum resident blocks of 128 threads per SM, which caps the
+// registers (2: about 254, 8 warps per SM; 4: 128, 16 warps, a few spills);
+// the variant is chosen once per process by timing (cvc_pi_variant).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_cvc_pi(double *__restrict__ conn,
                                                 const double2 *__restrict__ P0,
                                                 const double2 *__restrict__ P1,
                                                 const double2 *__restrict__ Z,
@@ -342,6 +346,8 @@ static int conn_out(cvcb_lattice *L, double *dst, const double *src, size_t ndou
   return CVCB_OK;
 }
 
+static int g_cvc_pi_variant = -1;
+
 int cvc_contract(cvcb_lattice *L, const double *const *fields, int src, double *conn,
                  double *contact) {
   CVCB_TRY(need_gauge(L));
@@ -369,13 +375,37 @@ int cvc_contract(cvcb_lattice *L, const double *const *fields, int src, double *
   gamma_tables(perm, sign);
   make_zplans(L, src, plans, Us, nullptr);
   const int blocks = (g.V + 127) / 128;
+  auto pi = [&](int v, int nu) {
+    double *c = static_cast<double *>(cb);
+    const double2 *P1 = P + (size_t)nu * 12 * fs, *Z = static_cast<const double2 *>(zb);
+    switch (v) {
+      case 1: k_cvc_pi<3><<<blocks, 128, 0, L->stream>>>(c, P + 48 * fs, P1, Z, L->U64, g, nu); break;
+      case 2: k_cvc_pi<4><<<blocks, 128, 0, L->stream>>>(c, P + 48 * fs, P1, Z, L->U64, g, nu); break;
+      default: k_cvc_pi<2><<<blocks, 128, 0, L->stream>>>(c, P + 48 * fs, P1, Z, L->U64, g, nu); break;
+    }
+  };
   for (int nu = 0; nu < 4; ++nu) {
     const ZPlan &plan = plans[nu];
     k_cvc_z<<<blocks, 128, 0, L->stream>>>(static_cast<double2 *>(zb), P + 60 * fs, plan, g.V);
     CVCB_LAUNCHED(L);
-    k_cvc_pi<<<blocks, 128, 0, L->stream>>>(static_cast<double *>(cb), P + 48 * fs,
-                                            P + (size_t)nu * 12 * fs,
-                                            static_cast<const double2 *>(zb), L->U64, g, nu);
+    if (g_cvc_pi_variant < 0) {  // first use in this process: time the variants (same results)
+      cudaEvent_t e0, e1;
+      CVCB_CUDA(cudaEventCreate(&e0));
+      CVCB_CUDA(cudaEventCreate(&e1));
+      float best = 1e30f;
+      for (int v = 0; v < 3; ++v) {
+        CVCB_CUDA(cudaEventRecord(e0, L->stream));
+        pi(v, nu);
+        CVCB_CUDA(cudaEventRecord(e1, L->stream));
+        CVCB_CUDA(cudaEventSynchronize(e1));
+        float ms;
+        CVCB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) best = ms, g_cvc_pi_variant = v;
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    }
+    pi(g_cvc_pi_variant, nu);
     CVCB_LAUNCHED(L);
   }
   CVCB_TRY(conn_out(L, conn, static_cast<const double *>(cb), (size_t)g.V * 32));
