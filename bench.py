@@ -115,9 +115,10 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def stencil_traffic_from_profile(key):
-    """DRAM bytes per launch of the stencil from the committed ncu summary
-    (profiles/*.md lines 'traffic <key> <bytes>'), or None."""
+def stencil_traffic_ratio(key):
+    """DRAM bytes over algorithmic bytes of the stencil from the committed ncu
+    summary of the same kernel and batch (profiles/*.md lines
+    'traffic_ratio <key> <ratio>'), or None."""
     pdir = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pdir):
         return None
@@ -126,7 +127,7 @@ def stencil_traffic_from_profile(key):
             continue
         for line in open(os.path.join(pdir, fn)):
             f = line.strip().strip("`").split()
-            if len(f) == 3 and f[0] == "traffic" and f[1] == key:
+            if len(f) == 3 and f[0] == "traffic_ratio" and f[1] == key:
                 return float(f[2])
     return None
 
@@ -390,7 +391,8 @@ def main():
     shape = [ctypes.c_int() for _ in range(4)]
     lat._lib.cvcb_tuned_shape(lat._h, prec, params.link_recon, nb, *[ctypes.byref(v) for v in shape])
     traffic_key = f"{args.precision}-{params.link_recon}-n{nb}-{T}x{LX}x{LY}x{LZ}"
-    traffic = stencil_traffic_from_profile(traffic_key)
+    ratio = stencil_traffic_ratio(traffic_key)
+    traffic = ratio * stencil_bytes if ratio and pl.value else None
 
     result = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
@@ -418,6 +420,9 @@ def main():
                       f"{args.precision}, {params.link_recon}-real links)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "traffic_source": "DRAM bytes / algorithmic bytes of the same kernel from its ncu "
+                              "capture (profiles/), times this run's algorithmic bytes per launch"
+                              if traffic else None,
             "peak_source": peak_kind, "launches_timed": pl.value,
             "avg_launch_ms": stencil_avg_ms, "algorithmic_bytes_per_launch": stencil_bytes,
         },

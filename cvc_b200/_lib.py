@@ -84,6 +84,7 @@ SIGNATURES = {
     "cvcb_solve": (_I, [_P, _P, _P, _I, ctypes.POINTER(SolverParams), ctypes.POINTER(SolverStats)]),
     "cvcb_time_stencil": (_I, [_P, _I, _I, _I, _I, _I, _DP]),
     "cvcb_sloppy_normal_op": (_I, [_P, _I, _I, _I, _I, _P, _P]),
+    "cvcb_time_link_product": (_I, [_P, _I, _I, _DP, _DP]),
     "cvcb_tuned_shape": (_I, [_P, _I, _I, _I, _IP, _IP, _IP, _IP]),
     "cvcb_profile": (_I, [_P, _I]),
     "cvcb_counters": (_I, [_P, _P, _P, _P, _P]),

@@ -270,6 +270,17 @@ int cvcb_time_stencil(cvcb_lattice *lat, int kind, int precision, int link_recon
 int cvcb_sloppy_normal_op(cvcb_lattice *lat, int precision, int link_recon, int layout, int nrhs,
                           const double *const *in, double *const *out);
 
+/* Tensor-core trial of the stencil's link product (u = W h for the 8 links
+ * of every site of a half lattice and one block of 2 spins x 12 right-hand
+ * sides, summed): variant 0 packed FP32x2 FMAs as the stencil does it,
+ * 1 mma.sync TF32 with two sites per block-diagonal tile, 2 the same with
+ * three TF32 products (FP32 accuracy).  Returns the average time of `reps`
+ * launches and the largest deviation from variant 0 relative to the largest
+ * component.  For the record of the trial; the stencil uses variant 0.  No
+ * counterpart in the reference. */
+int cvcb_time_link_product(cvcb_lattice *lat, int variant, int reps, double *ms,
+                           double *rel_diff);
+
 /* Launch shape the autotuner chose for the batched stencil for this lattice
  * volume, precision, link format and batch size: sites per thread block,
  * thread rows per block (each row a group of right-hand sides), right-hand
