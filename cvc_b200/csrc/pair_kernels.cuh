@@ -135,8 +135,6 @@ struct LT32c {
   }
 };
 
-inline size_t lt_tiles(int V) { return (size_t)(V + kTile - 1) / kTile; }
-
 // h = (1 + s g_mu) f projected to spins 0, 1, both rhs (table in
 // spinor_ops.cuh); with g5 on the input the sign of the lower spins flips
 template <int MU, int S>
