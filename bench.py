@@ -216,7 +216,7 @@ def reference_rate(pool, warmup, steps, n_conv=None):
     unless given.  A run with niter_max = n costs (n + 1 + c) iterations,
     c the fixed part (the initial residual and the final Qf5); c comes from
     runs of 1 and 3 iterations, after which each step is one bounded round
-    of 2 iterations per worker."""
+    of 1 iteration per worker."""
     full = None
     if n_conv is None:
         wall, res = pool.run(20000)
@@ -234,9 +234,9 @@ def reference_rate(pool, warmup, steps, n_conv=None):
     c = max(t1 / t_it - 1.0, 0.0)
     times, walls = [], []
     for i in range(warmup + steps):
-        wall, r = pool.run(1)
+        wall, r = pool.run(0)
         if i >= warmup:
-            times.append(max(dt for _, dt in r) / (2.0 + c))
+            times.append(max(dt for _, dt in r) / (1.0 + c))
             walls.append(wall)
     sec_it = float(np.mean(times))
     return {"value": pool.workers / (sec_it * n_conv), "sec_per_iteration": sec_it,
@@ -492,7 +492,7 @@ def main():
 
 def cpu_baseline_leg(result):
     """The unmodified reference invert_Qtm_her on one host core, a bounded
-    sample (runs of 1, 3 and 2 iterations on one column), extrapolated to
+    sample (runs of 1, 3 and 1 iterations on one column), extrapolated to
     the iteration count that the same algorithm needed on the GPU."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bind as ob
@@ -507,7 +507,7 @@ def cpu_baseline_leg(result):
         pool.close()
     return {"value": r["value"], "unit": "solves/s", "cores": 1, "kind": "reference",
             "sample": f"unmodified invert_Qtm_her (oracle/_ref, serial) on one 24^3x48 "
-                      f"point-source column: bounded runs of 1, 3 and 2 iterations, "
+                      f"point-source column: bounded runs of 1, 3 and 1 iterations, "
                       f"{r['sec_per_iteration']:.2f} s per iteration, extrapolated to "
                       f"{r['n_conv']:.1f} iterations per solve "
                       + ("(the count the same algorithm needed on the GPU)" if its else
@@ -519,7 +519,7 @@ def run_reference_arm(args):
     invert_Qtm_her per worker process, each on its own column of the
     workload.  Before the steps every worker solves its column to the
     benchmark's residual, which measures the iteration count; each step is
-    then one bounded round (2 iterations per worker), and the rate is
+    then one bounded round (1 iteration per worker), and the rate is
     workers / (seconds per iteration x iterations to convergence)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bind as ob
@@ -554,8 +554,8 @@ def run_reference_arm(args):
                 "sec_per_iteration": r["sec_per_iteration"], "full_solves": r["full"],
                 "total_s": time.perf_counter() - t_start},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "reference",
-                         "sample": f"{workers} processes, each step one round of 2 "
-                                   f"invert_Qtm_her iterations per process "
+                         "sample": f"{workers} processes, each step one round of 1 "
+                                   f"invert_Qtm_her iteration per process "
                                    f"({r['sec_per_iteration']:.2f} s per iteration), "
                                    f"{r['n_conv']:.1f} iterations per solve ({how}); "
                                    f"host has {cores} cores"},
