@@ -237,6 +237,204 @@ __global__ void k_p_upd_pt(P32 p, P32 rs, P32 xs, Scal S, int nsites, int nrhs) 
   store_active(p, blockIdx.y, s, pv, act_a, act_b);
 }
 
+// Pair-tiled forms of the reliable-update kernels below: thread = site x rhs
+// pair, so each pair-tiled field is read once (the per-rhs forms read both
+// lanes of every float4 for one rhs).  skip[r] != 0 leaves rhs r unchanged.
+struct PairLanes {
+  int ra;
+  bool has_b, act_a, act_b;
+};
+__device__ __forceinline__ PairLanes pair_lanes(int pr, int nrhs, const int *skip) {
+  PairLanes m;
+  m.ra = 2 * pr;
+  m.has_b = m.ra + 1 < nrhs;
+  m.act_a = !(skip && skip[m.ra]);
+  m.act_b = m.has_b && !(skip && skip[m.ra + 1]);
+  return m;
+}
+__device__ __forceinline__ float lane_re(const CP &c, int l) { return l ? c.re.y : c.re.x; }
+__device__ __forceinline__ float lane_im(const CP &c, int l) { return l ? c.im.y : c.im.x; }
+
+// x64 += x_s / scale; x_s = 0
+__global__ void k_absorb_pt(F64Acc x64, P32 xs, const double *scale, const int *skip, int nsites,
+                            int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pr = blockIdx.y;
+  const PairLanes m = pair_lanes(pr, nrhs, skip);
+  if (s >= nsites || (!m.act_a && !m.act_b)) return;
+  const SpinorPair v = xs.load_pair(pr, s);
+#pragma unroll
+  for (int l = 0; l < 2; ++l) {
+    if (!(l ? m.act_b : m.act_a)) continue;
+    const int r = m.ra + l;
+    const double w = 1.0 / scale[r];
+    Spinor<double> xv = x64.load(r, s);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        xv.c[k][c].re = fma(w, (double)lane_re(v.c[k][c], l), xv.c[k][c].re);
+        xv.c[k][c].im = fma(w, (double)lane_im(v.c[k][c], l), xv.c[k][c].im);
+      }
+    x64.store(r, s, xv);
+  }
+  SpinorPair z;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) z.c[k][c].re = z.c[k][c].im = make_float2(0.f, 0.f);
+  store_active(xs, pr, s, z, m.act_a, m.act_b);
+}
+
+// sloppy <- scale * FP64
+__global__ void k_to_sloppy_pt(P32 dst, F64Acc src, const double *scale, const int *skip,
+                               int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pr = blockIdx.y;
+  const PairLanes m = pair_lanes(pr, nrhs, skip);
+  if (s >= nsites || (!m.act_a && !m.act_b)) return;
+  SpinorPair o;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.c[k][c].re = o.c[k][c].im = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int l = 0; l < 2; ++l) {
+    if (!(l ? m.act_b : m.act_a)) continue;
+    const int r = m.ra + l;
+    const double w = scale[r];
+    const Spinor<double> v = src.load(r, s);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float re = (float)(w * v.c[k][c].re), im = (float)(w * v.c[k][c].im);
+        if (l) {
+          o.c[k][c].re.y = re;
+          o.c[k][c].im.y = im;
+        } else {
+          o.c[k][c].re.x = re;
+          o.c[k][c].im.x = im;
+        }
+      }
+  }
+  store_active(dst, pr, s, o, m.act_a, m.act_b);
+}
+
+// p = p - r_s (the kept direction q, see k_dir_strip)
+__global__ void k_dir_strip_pt(P32 p, P32 rs, const int *skip, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pr = blockIdx.y;
+  const PairLanes m = pair_lanes(pr, nrhs, skip);
+  if (s >= nsites || (!m.act_a && !m.act_b)) return;
+  SpinorPair pv = p.load_pair(pr, s);
+  const SpinorPair rv = rs.load_pair(pr, s);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      pv.c[k][c].re = sub2(pv.c[k][c].re, rv.c[k][c].re);
+      pv.c[k][c].im = sub2(pv.c[k][c].im, rv.c[k][c].im);
+    }
+  store_active(p, pr, s, pv, m.act_a, m.act_b);
+}
+
+// p = (a - i b) r_s' + u q, per-lane coefficients as in k_dir_restore
+__global__ void k_dir_restore_pt(P32 p, P32 rs, Scal S, const int *skip, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pr = blockIdx.y;
+  const PairLanes m = pair_lanes(pr, nrhs, skip);
+  if (s >= nsites || (!m.act_a && !m.act_b)) return;
+  float ca[2] = {1.f, 1.f}, cb[2] = {0.f, 0.f}, cu[2] = {0.f, 0.f};
+#pragma unroll
+  for (int l = 0; l < 2; ++l) {
+    if (!(l ? m.act_b : m.act_a)) continue;
+    const int r = m.ra + l;
+    const double u = S.scale[r] / S.scale_prev[r];
+    const double n2 = S.rr[r], cre = u * S.pAp[r], cim = u * S.alpha[r];
+    const bool ok = n2 > 0 && isfinite(n2) && isfinite(cre) && isfinite(cim) && isfinite(u);
+    ca[l] = (float)(ok ? 1.0 - cre / n2 : 1.0);
+    cb[l] = (float)(ok ? cim / n2 : 0.0);
+    cu[l] = (float)(ok ? u : 0.0);
+  }
+  const float2 a = make_float2(ca[0], ca[1]), b = make_float2(cb[0], cb[1]),
+               uq = make_float2(cu[0], cu[1]);
+  SpinorPair pv = p.load_pair(pr, s);
+  const SpinorPair rv = rs.load_pair(pr, s);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const CP x = rv.c[k][c];
+      // re = uq q.re + a x.re + b x.im ; im = uq q.im + a x.im - b x.re
+      float2 re = __fmul2_rn(uq, pv.c[k][c].re), im = __fmul2_rn(uq, pv.c[k][c].im);
+      re = __ffma2_rn(a, x.re, re);
+      re = __ffma2_rn(b, x.im, re);
+      im = __ffma2_rn(a, x.im, im);
+      im = __ffma2_rn(make_float2(-b.x, -b.y), x.re, im);
+      pv.c[k][c].re = re;
+      pv.c[k][c].im = im;
+    }
+  store_active(p, pr, s, pv, m.act_a, m.act_b);
+}
+
+__global__ void k_copy_pt(P32 dst, P32 src, const int *skip, int nsites, int nrhs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pr = blockIdx.y;
+  const PairLanes m = pair_lanes(pr, nrhs, skip);
+  if (s >= nsites || (!m.act_a && !m.act_b)) return;
+  store_active(dst, pr, s, src.load_pair(pr, s), m.act_a, m.act_b);
+}
+
+// <a, b> = sum conj(a) b per rhs, real and imaginary parts from one pass:
+// blockIdx.y = pair; partials[(2 rhs + part) * kMaxRedBlocks + block]
+// (part 0 real, 1 imaginary); the last block writes re[r], im[r].
+__global__ void __launch_bounds__(kRedThreads)
+    k_cdot_pt(P32 a, P32 b, int nsites, int nrhs, double *partials, unsigned *counters,
+              const int *__restrict__ skip, double *re, double *im) {
+  const int pr = blockIdx.y;
+  const PairLanes m = pair_lanes(pr, nrhs, skip);
+  if (!m.act_a && !m.act_b) return;
+  __shared__ double sh[4][kRedThreads / 32];
+  __shared__ bool last;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};  // re a, im a, re b, im b
+  for (int s = blockIdx.x * kRedThreads + threadIdx.x; s < nsites; s += gridDim.x * kRedThreads) {
+    const SpinorPair u = a.load_pair(pr, s), w = b.load_pair(pr, s);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const CP &x = u.c[k][c], &y = w.c[k][c];
+        v[0] += (double)x.re.x * y.re.x + (double)x.im.x * y.im.x;
+        v[1] += (double)x.re.x * y.im.x - (double)x.im.x * y.re.x;
+        v[2] += (double)x.re.y * y.re.y + (double)x.im.y * y.im.y;
+        v[3] += (double)x.re.y * y.im.y - (double)x.im.y * y.re.y;
+      }
+  }
+  block_sum<4>(v, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      partials[((size_t)2 * m.ra + q) * kMaxRedBlocks + blockIdx.x] = v[q];
+    __threadfence();
+    last = atomicAdd(counters + pr, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = 0.0;
+  for (int blk = threadIdx.x; blk < (int)gridDim.x; blk += kRedThreads)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] += __ldcg(partials + ((size_t)2 * m.ra + q) * kMaxRedBlocks + blk);
+  block_sum<4>(v, sh);
+  if (threadIdx.x == 0) {
+    counters[pr] = 0;
+    if (m.act_a) re[m.ra] = v[0], im[m.ra] = v[1];
+    if (m.act_b) re[m.ra + 1] = v[2], im[m.ra + 1] = v[3];
+  }
+}
+
 // Reliable update, step 1: x64 += x_s / scale; x_s = 0 (rhs with skip[r] == 0)
 template <class XF>
 __global__ void k_absorb(F64Acc x64, XF xs, const double *scale, const int *skip, int nsites,
@@ -814,7 +1012,11 @@ struct Batch {
   int reliable_update(bool absorb) {
     dim3 eg((g.Vh + 127) / 128, n);
     if (absorb) {
-      k_absorb<<<eg, 128, 0, L->stream>>>(f64(x64, 1), xs, S.scale, ru_skip, g.Vh, n);
+      if constexpr (std::is_same<XF, P32>::value)
+        k_absorb_pt<<<dim3(eg.x, (n + 1) / 2), 128, 0, L->stream>>>(f64(x64, 1), xs, S.scale,
+                                                                    ru_skip, g.Vh, n);
+      else
+        k_absorb<<<eg, 128, 0, L->stream>>>(f64(x64, 1), xs, S.scale, ru_skip, g.Vh, n);
       CVCB_LAUNCHED(L);
       CVCB_TRY(schur64(y64, x64, mu, ru_skip));
     } else {
@@ -824,7 +1026,11 @@ struct Batch {
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedRhat{f64(bh64, 1), f64(y64, 1)},
                                                     EpiRhat{S}, g.Vh, br, ru_skip);
     CVCB_LAUNCHED(L);
-    k_to_sloppy<<<eg, 128, 0, L->stream>>>(yo, f64(y64, 1), S.scale, ru_skip, g.Vh, n);
+    if constexpr (std::is_same<SF, P32>::value)
+      k_to_sloppy_pt<<<dim3(eg.x, (n + 1) / 2), 128, 0, L->stream>>>(yo, f64(y64, 1), S.scale,
+                                                                      ru_skip, g.Vh, n);
+    else
+      k_to_sloppy<<<eg, 128, 0, L->stream>>>(yo, f64(y64, 1), S.scale, ru_skip, g.Vh, n);
     CVCB_LAUNCHED(L);
     CVCB_TRY(dag_sloppy(rs, yo, ru_skip));
     k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedNormS<SF>{rs}, EpiRR{S}, g.Vh, br, ru_skip);
@@ -939,7 +1145,7 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   const size_t nrm = sizeof(float) * (size_t)g.Vh * n;
   auto rnd = [](size_t b) { return (b + 255) & ~size_t(255); };  // every piece 256-aligned
   const size_t scal = 8 * rnd(sizeof(double) * kMaxBatch) + 3 * rnd(sizeof(int) * kMaxBatch);
-  const size_t part = rnd(sizeof(double) * kMaxRedBlocks * kMaxBatch) +
+  const size_t part = rnd(sizeof(double) * kMaxRedBlocks * kMaxBatch * 2) +
                       rnd(sizeof(unsigned) * kMaxBatch);
   const size_t dotb = sizeof(double) * (size_t)n * (g.Vh / 32 + 64);
   const size_t total = 5 * rnd(f64) + 6 * (rnd(sl) + rnd(nrm)) + rnd(xsl) + rnd(nrm) + scal + part +
@@ -981,7 +1187,7 @@ int setup_batch(cvcb_lattice *L, Batch<SF, XF, LF> &B, int n, bool with_fp64 = t
   B.S.done = (int *)take(sizeof(int) * kMaxBatch);
   B.ru_skip = (int *)take(sizeof(int) * kMaxBatch);
   B.rst_skip = (int *)take(sizeof(int) * kMaxBatch);
-  B.br.partials = (double *)take(sizeof(double) * kMaxRedBlocks * kMaxBatch);
+  B.br.partials = (double *)take(sizeof(double) * kMaxRedBlocks * kMaxBatch * 2);
   B.br.counters = (unsigned *)take(sizeof(unsigned) * kMaxBatch);
   B.dot_part = (double *)take(dotb);
   B.err = (int *)take(sizeof(int));
@@ -1169,7 +1375,10 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
   CVCB_TRY(B.reliable_update(false));
   // x_s = 0 (all-zero bits are 0.0), p = r_s
   CVCB_CUDA(cudaMemsetAsync(B.xs_mem, 0, B.xs_bytes, L->stream));
-  k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, nullptr, g.Vh, n);
+  if constexpr (std::is_same<SF, P32>::value)
+    k_copy_pt<<<dim3(eg.x, (n + 1) / 2), 128, 0, L->stream>>>(B.p, B.rs, nullptr, g.Vh, n);
+  else
+    k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, nullptr, g.Vh, n);
   CVCB_LAUNCHED(L);
   std::vector<double> rr(n), rr_max(n), rhat2(n), ratio2(n), target2(n);
   std::vector<int> done(n, 0), iters(n, 0), since(n, 0), skip(n, 0), rst(n, 1);
@@ -1322,16 +1531,27 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     CVCB_TRY(put_flags(L, B.ru_skip, skip, n));
     // keep the search direction: q = p - r_s now, p = r_s' + q (q orthogonalised
     // against r_s') after the update
-    k_dir_strip<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.ru_skip, g.Vh, n);
+    const dim3 egp(eg.x, (n + 1) / 2);  // pair-tiled fields: one thread per site and pair
+    if constexpr (std::is_same<SF, P32>::value)
+      k_dir_strip_pt<<<egp, 128, 0, L->stream>>>(B.p, B.rs, B.ru_skip, g.Vh, n);
+    else
+      k_dir_strip<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.ru_skip, g.Vh, n);
     CVCB_LAUNCHED(L);
     CVCB_TRY(B.reliable_update(true));
-    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedCdot<SF>{B.rs, B.p, 0}, EpiStore{B.S.pAp},
-                                                    g.Vh, B.br, B.ru_skip);
-    CVCB_LAUNCHED(L);
-    k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedCdot<SF>{B.rs, B.p, 1},
-                                                    EpiStore{B.S.alpha}, g.Vh, B.br, B.ru_skip);
-    CVCB_LAUNCHED(L);
-    k_dir_restore<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.S, B.ru_skip, g.Vh, n);
+    if constexpr (std::is_same<SF, P32>::value) {
+      k_cdot_pt<<<dim3(rg.x, (n + 1) / 2), kRedThreads, 0, L->stream>>>(
+          B.rs, B.p, g.Vh, n, B.br.partials, B.br.counters, B.ru_skip, B.S.pAp, B.S.alpha);
+      CVCB_LAUNCHED(L);
+      k_dir_restore_pt<<<egp, 128, 0, L->stream>>>(B.p, B.rs, B.S, B.ru_skip, g.Vh, n);
+    } else {
+      k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedCdot<SF>{B.rs, B.p, 0},
+                                                      EpiStore{B.S.pAp}, g.Vh, B.br, B.ru_skip);
+      CVCB_LAUNCHED(L);
+      k_reduce_rhs<<<rg, kRedThreads, 0, L->stream>>>(RedCdot<SF>{B.rs, B.p, 1},
+                                                      EpiStore{B.S.alpha}, g.Vh, B.br, B.ru_skip);
+      CVCB_LAUNCHED(L);
+      k_dir_restore<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.S, B.ru_skip, g.Vh, n);
+    }
     CVCB_LAUNCHED(L);
     // a residual that stopped being finite restarts from the recomputed one
     bool restart = false;
@@ -1341,7 +1561,10 @@ int run_batch(cvcb_lattice *L, double *const *x, const double *const *b, int n,
     }
     if (restart) {
       CVCB_TRY(put_flags(L, B.rst_skip, rst, n));
-      k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.rst_skip, g.Vh, n);
+      if constexpr (std::is_same<SF, P32>::value)
+        k_copy_pt<<<egp, 128, 0, L->stream>>>(B.p, B.rs, B.rst_skip, g.Vh, n);
+      else
+        k_copy<<<eg, 128, 0, L->stream>>>(B.p, B.rs, B.rst_skip, g.Vh, n);
       CVCB_LAUNCHED(L);
       for (int i = 0; i < n; ++i) nrestart += !rst[i];
     }
