@@ -408,14 +408,17 @@ def main():
             "stencil_shape": {"sites_per_block": shape[0].value, "rows_per_block": shape[1].value,
                               "rhs_per_thread": shape[2].value,
                               "variant": ["per-thread links", "shared-memory links",
-                                          "packed FP32x2 rhs pairs",
-                                          "pair-tiled fields"][shape[3].value]},
+                                          "packed FP32x2 rhs pairs", "pair-tiled fields",
+                                          "pair-tiled fields, TMEM accumulator",
+                                          "pair-tiled fields, TMEM accumulator, pipelined",
+                                          "pair-tiled fields, bulk-staged t/x neighbours"]
+                                         [shape[3].value]},
             "inner_iterations_per_step": iters // max(args.steps, 1),
             "max_true_residual": worst_res,
         },
         "roofline": {
-            "kernel": ["k_eo_hop", "k_eo_hop_staged", "k_eo_hop_x2",
-                       "k_eo_hop_pt"][shape[3].value] +
+            "kernel": ["k_eo_hop", "k_eo_hop_staged", "k_eo_hop_x2", "k_eo_hop_pt",
+                       "k_eo_hop_ptm", "k_eo_hop_ptm", "k_eo_hop_ptb"][shape[3].value] +
                       " (batched even/odd stencil sweep, "
                       f"{args.precision}, {params.link_recon}-real links)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -111,6 +111,24 @@ struct LT32f {
     }
     return L;
   }
+  // the loaded words and the link built from them, separately (so that a
+  // kernel can issue the loads early and build the link when it needs it)
+  struct Raw {
+    float2 v[9];
+  };
+  __device__ __forceinline__ Raw load_raw(int mu, int idx) const {
+    const float2 *q = U + (size_t)(idx >> 5) * (36 * kTile) + mu * 9 * kTile + (idx & (kTile - 1));
+    Raw r;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) r.v[k] = __ldg(q + k * kTile);
+    return r;
+  }
+  __device__ __forceinline__ Link<float> build(const Raw &r, int) const {
+    Link<float> L;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) L.m[k / 3][k % 3] = cx(r.v[k].x, r.v[k].y);
+    return L;
+  }
 };
 
 // 12-real phased links (rows 0, 1), tiled: float4 U[idx / 32][mu][3][idx % 32];
@@ -128,6 +146,27 @@ struct LT32c {
       const float4 v = __ldg(q + k * kTile);
       L.m[(2 * k) / 3][(2 * k) % 3] = cx(v.x, v.y);
       L.m[(2 * k + 1) / 3][(2 * k + 1) % 3] = cx(v.z, v.w);
+    }
+    reconstruct_row2(L);
+    apply_row2_phase(L, ph[mu]);
+    return L;
+  }
+  struct Raw {
+    float4 v[3];
+  };
+  __device__ __forceinline__ Raw load_raw(int mu, int idx) const {
+    const float4 *q = U + (size_t)(idx >> 5) * (12 * kTile) + mu * 3 * kTile + (idx & (kTile - 1));
+    Raw r;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r.v[k] = __ldg(q + k * kTile);
+    return r;
+  }
+  __device__ __forceinline__ Link<float> build(const Raw &r, int mu) const {
+    Link<float> L;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      L.m[(2 * k) / 3][(2 * k) % 3] = cx(r.v[k].x, r.v[k].y);
+      L.m[(2 * k + 1) / 3][(2 * k + 1) % 3] = cx(r.v[k].z, r.v[k].w);
     }
     reconstruct_row2(L);
     apply_row2_phase(L, ph[mu]);
@@ -313,6 +352,297 @@ __global__ void __launch_bounds__(kHopMaxThreads, 2) k_eo_hop_pt(HopArgs<P32, LF
   }
 }
 
+// ---- the same sweep with the accumulator in tensor memory --------------------
+// The register budget of k_eo_hop_pt (a 48-register two-rhs accumulator, the
+// 60 registers of one direction's loads) caps it at 16 warps per SM, and the
+// sweep is bound by load latency at that occupancy.  Here the accumulator
+// lives in tensor memory (TMEM, 512 columns x 128 lanes of 32 bits per SM):
+// thread = lane of its warp's 32-lane quarter (warp w of a 128-thread block
+// owns lanes 32 w .. 32 w + 31), component k = 3 spin + colour of the site's
+// two-rhs spinor at columns 4 k .. 4 k + 3 = (re a, re b, im a, im b).  Each
+// direction adds its reconstructed contribution with tcgen05.ld / add /
+// tcgen05.st in three 16-column chunks, component by component in the same
+// order as the register accumulator (the results are bitwise those of
+// k_eo_hop_pt).  The freed registers buy either more warps (PIPE false: 80
+// registers, 24 warps per SM) or the next direction's loads in flight while
+// one direction is computed (PIPE true: 128 registers, 16 warps).
+// Each block allocates 64 columns (48 used) once and frees them before it
+// exits; at most 8 blocks of this kernel fit the 512 columns of an SM, and
+// both register budgets keep residency at or below that (6 and 4 blocks).
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+constexpr int kTmemThreads = 128;
+constexpr int kTmemCols = 64;
+
+__device__ __forceinline__ void tmem_ld16(unsigned a, float (&v)[16]) {
+  unsigned r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(a));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+__device__ __forceinline__ void tmem_st16(unsigned a, const float (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16};" ::"r"(a),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// component (s, c) of the (1 + S g_mu)-reconstruction of u added to a (the
+// table of accum_recon_pair, one component)
+template <int MU, int S>
+__device__ __forceinline__ void recon_add(CP &a, int s, int c, const HalfPair &u) {
+  if (s < 2) {
+    a.re = add2(a.re, u.c[s][c].re);
+    a.im = add2(a.im, u.c[s][c].im);
+  } else if (MU == 0) {  // r2 = -S u0, r3 = -S u1
+    const CP &v = u.c[s - 2][c];
+    a.re = S > 0 ? sub2(a.re, v.re) : add2(a.re, v.re);
+    a.im = S > 0 ? sub2(a.im, v.im) : add2(a.im, v.im);
+  } else if (MU == 1) {  // r2 = S i u1, r3 = S i u0
+    const CP &v = u.c[s == 2 ? 1 : 0][c];
+    a.re = S > 0 ? sub2(a.re, v.im) : add2(a.re, v.im);
+    a.im = S > 0 ? add2(a.im, v.re) : sub2(a.im, v.re);
+  } else if (MU == 2) {  // r2 = S u1, r3 = -S u0
+    const CP &v = u.c[s == 2 ? 1 : 0][c];
+    const bool plus = (s == 2) == (S > 0);
+    a.re = plus ? add2(a.re, v.re) : sub2(a.re, v.re);
+    a.im = plus ? add2(a.im, v.im) : sub2(a.im, v.im);
+  } else {  // r2 = S i u0, r3 = -S i u1
+    const CP &v = u.c[s - 2][c];
+    const bool plus = (s == 2) == (S > 0);  // a += i v
+    a.re = plus ? sub2(a.re, v.im) : add2(a.re, v.im);
+    a.im = plus ? add2(a.im, v.re) : sub2(a.im, v.re);
+  }
+}
+
+// acc (tensor memory, this thread's lane from column tacc) += reconstruction
+// of u; FIRST: the accumulator starts from zero (nothing loaded)
+template <int MU, int S, bool FIRST>
+__device__ __forceinline__ void tmem_accum(unsigned tacc, const HalfPair &u) {
+  if (!FIRST) tmem_wait_st();  // the previous direction's stores are complete
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    float v[16];
+    if (FIRST) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) v[k] = 0.f;
+    } else {
+      tmem_ld16(tacc + 16 * q, v);
+    }
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const int k = 4 * q + kk;
+      CP a;
+      a.re = make_float2(v[4 * kk], v[4 * kk + 1]);
+      a.im = make_float2(v[4 * kk + 2], v[4 * kk + 3]);
+      recon_add<MU, S>(a, k / 3, k % 3, u);
+      v[4 * kk] = a.re.x;
+      v[4 * kk + 1] = a.re.y;
+      v[4 * kk + 2] = a.im.x;
+      v[4 * kk + 3] = a.im.y;
+    }
+    tmem_st16(tacc + 16 * q, v);
+  }
+}
+
+// the loads of direction D (mu = 3, 3, 2, 2, 1, 1, 0, 0: z, y, x, t;
+// backward for even D, forward for odd D: the order of hop_pair_dir)
+template <class LF>
+struct DirLoads {
+  SpinorPair f;
+  typename LF::Raw w;
+};
+template <int D, class LF>
+__device__ __forceinline__ DirLoads<LF> load_dir(const HopArgs<P32, LF> &A, const SiteCoord &cd,
+                                                 int pr, int self, int qoff) {
+  constexpr int MU = 3 - (D >> 1);
+  constexpr int DIR = (D & 1) ? 1 : -1;
+  const int j = nb_lex(A.eg.g, cd, MU, DIR) >> 1;
+  DirLoads<LF> d;
+  d.w = A.links.load_raw(MU, DIR < 0 ? qoff + j : self);
+  d.f = A.in.load_pair(pr, j);
+  return d;
+}
+template <int D, class LF>
+__device__ __forceinline__ void apply_dir(unsigned tacc, const HopArgs<P32, LF> &A,
+                                          const DirLoads<LF> &d, bool g5in) {
+  constexpr int MU = 3 - (D >> 1);
+  const Link<float> W = A.links.build(d.w, MU);
+  if constexpr (D & 1) {  // forward: (1 - g_mu) U_mu(x) in(x+mu)
+    const HalfPair h = g5in ? project_pair<MU, +1>(d.f) : project_pair<MU, -1>(d.f);
+    tmem_accum<MU, -1, false>(tacc, link_mul_pair<false>(W, h));
+  } else {  // backward: (1 + g_mu) U_mu(x-mu)^+ in(x-mu)
+    const HalfPair h = g5in ? project_pair<MU, -1>(d.f) : project_pair<MU, +1>(d.f);
+    tmem_accum<MU, +1, D == 0>(tacc, link_mul_pair<true>(W, h));
+  }
+}
+
+// out component = D1 acc (+ D2 aux) per spin s, as diag_pair for one component
+__device__ __forceinline__ CP diag_comp(const CP &x, float a, float b) {
+  CP o;
+  o.re = __fmul2_rn(bc(a), x.re);
+  o.im = __fmul2_rn(bc(a), x.im);
+  o.re = __ffma2_rn(bc(-b), x.im, o.re);
+  o.im = __ffma2_rn(bc(b), x.re, o.im);
+  return o;
+}
+__device__ __forceinline__ void diag_comp_acc(CP &o, const CP &x, float a, float b) {
+  CP r;
+  r.re = __ffma2_rn(bc(a), x.re, o.re);
+  r.im = __ffma2_rn(bc(a), x.im, o.im);
+  r.re = __ffma2_rn(bc(-b), x.im, r.re);
+  r.im = __ffma2_rn(bc(b), x.re, r.im);
+  o = r;
+}
+
+template <class LF, bool G5IN, bool G5HOP, bool AUX, bool RUPD, bool PIPE>
+__global__ void __launch_bounds__(kTmemThreads, PIPE ? 4 : 6) k_eo_hop_ptm(HopArgs<P32, LF> A) {
+  const int pr = blockIdx.x;  // one rhs pair per block: every exit below is block-uniform
+  const int ra = 2 * pr;
+  if (ra >= A.nrhs) return;
+  const bool act_a = !(A.done && A.done[ra]);
+  const bool has_b = ra + 1 < A.nrhs;
+  const bool act_b = has_b && !(A.done && A.done[ra + 1]);
+  if (!act_a && !act_b) return;
+  __shared__ unsigned tm_base;
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tm_base)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  const unsigned tacc = tm_base + ((unsigned)(warp * 32) << 16);
+  const Geom &g = A.eg.g;
+  const int p = A.eg.p;
+  const int qoff = (1 - p) * g.Vh;
+  for (int sb = blockIdx.y; sb * kTmemThreads < g.Vh; sb += gridDim.y) {
+    const int i_raw = sb * kTmemThreads + threadIdx.x;
+    const bool valid = i_raw < g.Vh;  // the tensor-memory accesses need the whole warp
+    const int i = valid ? i_raw : g.Vh - 1;
+    const SiteCoord cd = site_coord(g, p, i);
+    const int self = p * g.Vh + i;
+    if constexpr (PIPE) {
+      DirLoads<LF> cur = load_dir<0>(A, cd, pr, self, qoff), nxt;
+      nxt = load_dir<1>(A, cd, pr, self, qoff);
+      apply_dir<0>(tacc, A, cur, G5IN);
+      cur = load_dir<2>(A, cd, pr, self, qoff);
+      apply_dir<1>(tacc, A, nxt, G5IN);
+      nxt = load_dir<3>(A, cd, pr, self, qoff);
+      apply_dir<2>(tacc, A, cur, G5IN);
+      cur = load_dir<4>(A, cd, pr, self, qoff);
+      apply_dir<3>(tacc, A, nxt, G5IN);
+      nxt = load_dir<5>(A, cd, pr, self, qoff);
+      apply_dir<4>(tacc, A, cur, G5IN);
+      cur = load_dir<6>(A, cd, pr, self, qoff);
+      apply_dir<5>(tacc, A, nxt, G5IN);
+      nxt = load_dir<7>(A, cd, pr, self, qoff);
+      apply_dir<6>(tacc, A, cur, G5IN);
+      apply_dir<7>(tacc, A, nxt, G5IN);
+    } else {
+      apply_dir<0>(tacc, A, load_dir<0>(A, cd, pr, self, qoff), G5IN);
+      apply_dir<1>(tacc, A, load_dir<1>(A, cd, pr, self, qoff), G5IN);
+      apply_dir<2>(tacc, A, load_dir<2>(A, cd, pr, self, qoff), G5IN);
+      apply_dir<3>(tacc, A, load_dir<3>(A, cd, pr, self, qoff), G5IN);
+      apply_dir<4>(tacc, A, load_dir<4>(A, cd, pr, self, qoff), G5IN);
+      apply_dir<5>(tacc, A, load_dir<5>(A, cd, pr, self, qoff), G5IN);
+      apply_dir<6>(tacc, A, load_dir<6>(A, cd, pr, self, qoff), G5IN);
+      apply_dir<7>(tacc, A, load_dir<7>(A, cd, pr, self, qoff), G5IN);
+    }
+    // epilogue, four components at a time: out = D1 (c [g5] hop) + D2 aux
+    // (or r -= alpha out), |out|^2 (or |r|^2) in FP64 in component order
+    const float2 na = RUPD ? make_float2(-(float)A.alpha[ra], has_b ? -(float)A.alpha[ra + 1] : 0.f)
+                           : make_float2(0.f, 0.f);
+    double2 n2 = make_double2(0.0, 0.0);
+    tmem_wait_st();
+    const float4 *auxp = AUX ? A.aux.at(pr, i) : nullptr;
+    float4 *dst = RUPD ? A.rup.at(pr, i) : A.out.at(pr, i);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      float v[16];
+      tmem_ld16(tacc + 16 * q, v);
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const int k = 4 * q + kk, s = k / 3;
+        const float g5 = s < 2 ? 1.f : -1.f;
+        const float gh = G5HOP ? g5 : 1.f;
+        CP x;
+        x.re = make_float2(v[4 * kk], v[4 * kk + 1]);
+        x.im = make_float2(v[4 * kk + 2], v[4 * kk + 3]);
+        CP o = diag_comp(x, (float)(A.c * A.d1a) * gh, (float)(A.c * A.d1b) * g5 * gh);
+        if (AUX) diag_comp_acc(o, cp_of(__ldg(auxp + k * kTile)), (float)A.d2a, (float)A.d2b * g5);
+        if (RUPD) {
+          CP rv = cp_of(__ldg(dst + k * kTile));
+          rv.re = __ffma2_rn(na, o.re, rv.re);
+          rv.im = __ffma2_rn(na, o.im, rv.im);
+          o = rv;
+        }
+        if (valid) {
+          if (A.dot_part) {
+            n2.x = fma((double)o.re.x, (double)o.re.x, n2.x);
+            n2.x = fma((double)o.im.x, (double)o.im.x, n2.x);
+            n2.y = fma((double)o.re.y, (double)o.re.y, n2.y);
+            n2.y = fma((double)o.im.y, (double)o.im.y, n2.y);
+          }
+          if (act_a && act_b) {
+            dst[k * kTile] = f4_of(o);
+          } else {
+            float *qf = reinterpret_cast<float *>(dst + k * kTile) + (act_a ? 0 : 1);
+            qf[0] = act_a ? o.re.x : o.re.y;
+            qf[2] = act_a ? o.im.x : o.im.y;
+          }
+        }
+      }
+    }
+    if (A.dot_part) {  // whole warps: the block width is a multiple of 32
+      double da = n2.x, db = n2.y;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        da += __shfl_down_sync(0xffffffffu, da, o);
+        db += __shfl_down_sync(0xffffffffu, db, o);
+      }
+      if ((threadIdx.x & 31) == 0) {
+        const int w = sb * (kTmemThreads >> 5) + warp;
+        A.dot_part[(size_t)ra * A.dot_np + w] = da;
+        if (has_b) A.dot_part[(size_t)(ra + 1) * A.dot_np + w] = db;
+      }
+    }
+  }
+  tmem_fence_before_sync();
+  __syncthreads();  // every warp's tensor-memory accesses are complete
+  tmem_fence_after_sync();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm_base),
+                 "r"(kTmemCols));
+}
+
 // ---- the same sweep with the t and x neighbours staged by bulk copies -------
 // On lattices with LY*LZ/2 a multiple of 32, the 32 sites of a tile share
 // their t and x coordinates, so the t+-, x+- neighbours of a tile are again
@@ -328,9 +658,6 @@ constexpr int kBulkWarps = 4;  // warps per block: 4 consecutive tiles of one rh
 constexpr unsigned kTileBytes = 12 * kTile * sizeof(float4);  // 6144
 constexpr size_t kBulkSmem = (size_t)kBulkWarps * 2 * kTileBytes;
 
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }

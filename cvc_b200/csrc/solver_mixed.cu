@@ -683,7 +683,8 @@ void mailbox(cvcb_lattice *L, int slot, std::vector<double> &out, int n) {
 // ---------------------------------------------------------------------------
 struct LaunchShape {
   int bx = 64, by = 1, nr = 1;  // sites per block, rhs groups per block, rhs per thread
-  int pk = 0;                   // 1: nr == 2 in packed FP32x2 arithmetic (k_eo_hop_x2)
+  int pk = 0;                   // 1: nr == 2 in packed FP32x2 arithmetic (k_eo_hop_x2, k_eo_hop_pt);
+                                // pair-tiled only: 2 k_eo_hop_ptb, 3 and 4 k_eo_hop_ptm
 };
 
 // Autotuner results, per process: (V, precision, recon, n) -> launch shape,
@@ -898,7 +899,9 @@ struct Batch {
   }
 
   // Pair-tiled stencil launch: pk 2 = bulk-staged t and x neighbours
-  // (k_eo_hop_ptb, whole-tile lattices only), else plain loads (k_eo_hop_pt)
+  // (k_eo_hop_ptb, whole-tile lattices only), pk 3, 4 = accumulator in
+  // tensor memory (k_eo_hop_ptm, 24 warps per SM / next direction's loads in
+  // flight), else plain loads (k_eo_hop_pt)
   template <class LL, bool G5IN, bool G5HOP, bool AUX, bool RUPD>
   int launch_pt(const HopArgs<P32, LL> &a, const LaunchShape &sh) {
     const int groups = (n + 1) / 2;
@@ -922,7 +925,18 @@ struct Batch {
       const int by = std::min(sh.by, groups);
       const int site_blocks = (g.Vh + sh.bx - 1) / sh.bx;
       dim3 block(sh.bx, by), grid((groups + by - 1) / by, std::min(site_blocks, 65535));
-      k_eo_hop_pt<LL, G5IN, G5HOP, AUX, RUPD><<<grid, block, 0, L->stream>>>(a);
+      if (sh.pk == 3 || sh.pk == 4) {  // accumulator in tensor memory: 128 sites, one pair per block
+        if (sh.bx != kTmemThreads || sh.by != 1) {
+          set_error("tensor-memory stencil needs 128 sites and one rhs pair per block");
+          return CVCB_ERR_ARG;
+        }
+        if (sh.pk == 3)
+          k_eo_hop_ptm<LL, G5IN, G5HOP, AUX, RUPD, false><<<grid, kTmemThreads, 0, L->stream>>>(a);
+        else
+          k_eo_hop_ptm<LL, G5IN, G5HOP, AUX, RUPD, true><<<grid, kTmemThreads, 0, L->stream>>>(a);
+      } else {
+        k_eo_hop_pt<LL, G5IN, G5HOP, AUX, RUPD><<<grid, block, 0, L->stream>>>(a);
+      }
     }
     CVCB_LAUNCHED(L);
     return CVCB_OK;
@@ -1251,8 +1265,11 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
       if (sizeof(typename SF::R) == 8) f.nr = 1, f.pk = 0;
       if (pairs) {  // pair-tiled fields: one rhs pair per thread; 4th field 2 = bulk-staged
         f.nr = 2;
-        f.pk = (nf >= 4 && f.pk == 2 && bulk_stencil_ok(L->g)) ? 2 : 1;
+        f.pk = (nf >= 4 && f.pk == 2 && bulk_stencil_ok(L->g)) ? 2
+               : (nf >= 4 && (f.pk == 3 || f.pk == 4))           ? f.pk
+                                                                 : 1;
         if (f.pk == 2) f.bx = kBulkWarps * 32, f.by = 1;
+        if (f.pk >= 3) f.bx = kTmemThreads, f.by = 1;
       }
       B.shape = f;
       g_tuned_shape[key] = f;
@@ -1291,6 +1308,18 @@ int tune_shape(cvcb_lattice *L, Batch<SF, XF, LF> &B, int prec, int recon, int b
         best = B.shape;
       }
     }
+  if (pairs) {  // the tensor-memory accumulator: one fixed block shape, two register budgets
+    for (int pk : {3, 4}) {
+      B.shape = LaunchShape{kTmemThreads, 1, 2, pk};
+      float ms;
+      if (time_ms(L, [&] { return B.normal_op_sloppy(B.Ap, B.p, nullptr); }, 3, &ms) != CVCB_OK) {
+        cudaGetLastError();
+      } else if (ms < best_ms) {
+        best_ms = ms;
+        best = B.shape;
+      }
+    }
+  }
   if (pairs && bulk_stencil_ok(L->g)) {  // the bulk-staged stencil: one fixed block shape
     B.shape = LaunchShape{kBulkWarps * 32, 1, 2, 2};
     float ms;
@@ -2014,7 +2043,7 @@ int cvcb_tuned_shape(cvcb_lattice *L, int precision, int link_recon, int nrhs, i
   *sites_per_block = s.bx;
   *rows_per_block = s.by;
   *rhs_per_thread = s.nr;
-  *variant = pairs ? 3 : s.pk ? 2 : (s.by > 1 && s.nr == 1) ? 1 : 0;
+  *variant = pairs ? (s.pk >= 3 ? 1 + s.pk : s.pk == 2 ? 6 : 3) : s.pk ? 2 : (s.by > 1 && s.nr == 1) ? 1 : 0;
   return CVCB_OK;
 }
 

@@ -286,8 +286,11 @@ int cvcb_time_link_product(cvcb_lattice *lat, int variant, int reps, double *ms,
  * thread rows per block (each row a group of right-hand sides), right-hand
  * sides per thread, and the kernel variant (0: links per thread, 1: links
  * staged in shared memory for all rows, 2: two rhs per thread in packed
- * FP32x2 arithmetic, 3: pair-tiled fields); CVCB_ERR_STATE before the first
- * tuning. */
+ * FP32x2 arithmetic, 3: pair-tiled fields, 4: pair-tiled fields with the
+ * accumulator in tensor memory at 80 registers, 5: the same at 128 registers
+ * with the next direction's loads in flight, 6: pair-tiled fields with the t
+ * and x neighbours staged in shared memory by bulk copies); CVCB_ERR_STATE
+ * before the first tuning. */
 int cvcb_tuned_shape(cvcb_lattice *lat, int precision, int link_recon, int nrhs,
                      int *sites_per_block, int *rows_per_block, int *rhs_per_thread,
                      int *variant);

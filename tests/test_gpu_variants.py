@@ -3,8 +3,9 @@ child process (the autotuner caches one shape per configuration and
 process): one rhs per thread with per-thread links, shared-memory links
 for several rows, 2 and 4 rhs per thread, packed FP32x2 rhs pairs, and
 (FP32 only, CVCB_PAIRS=1) the pair-tiled fields with 12- and 18-real
-links, with plain neighbour loads and with the t and x neighbours staged in
-shared memory by bulk copies (4th shape field 2).
+links, with plain neighbour loads, with the t and x neighbours staged in
+shared memory by bulk copies (4th shape field 2) and with the accumulator in
+tensor memory at both register budgets (4th shape field 3, 4).
 A wrong sloppy operator would still be corrected by the FP64 reliable
 updates, so each variant must also converge in the same number of inner
 iterations as the plain one (the arithmetic differs only in rounding)."""
@@ -45,7 +46,9 @@ print(json.dumps({"iters": st.iterations, "conv": st.converged, "res": st.max_tr
 VARIANTS = ["64,1,1", "32,4,1", "64,1,2", "32,1,4", "64,1,2,1", "32,2,2,1"]
 # (shape, CVCB_PAIRS, link reals) of the pair-tiled fields
 PAIR_VARIANTS = [("64,1,2,1", 1, 12), ("32,2,2,1", 1, 12), ("64,1,2,1", 1, 18),
-                 ("128,1,2,1", 1, 18), ("128,1,2,2", 1, 12), ("128,1,2,2", 1, 18)]
+                 ("128,1,2,1", 1, 18), ("128,1,2,2", 1, 12), ("128,1,2,2", 1, 18),
+                 ("128,1,2,3", 1, 12), ("128,1,2,3", 1, 18), ("128,1,2,4", 1, 12),
+                 ("128,1,2,4", 1, 18)]
 
 
 def run(prec, shape, pairs=0, recon=12):
