@@ -39,6 +39,9 @@ KAPPA = 0.155
 MU = 0.005 / (2 * KAPPA)
 EPS, SEED = 0.25, 11
 NSRC, TOL = 8, 1e-10
+# the P -> gamma gamma configuration: 32^3x64, kappa 0.156, 2 kappa mu 0.004,
+# eps 0.3 gauge field (seed 21), sequential source at separation 16
+C5_DIMS, C5_KAPPA, C5_MU2K, C5_EPS, C5_SEED, C5_DT = (64, 32, 32, 32), 0.156, 0.004, 0.3, 21, 16
 WORKLOAD = ("24^3x48 twisted-mass Wilson, kappa 0.155, 2*kappa*mu 0.005, eps 0.25 gauge "
             "(ranlxd seed 11), 8 point sources x 12 spin-colour = 96 rhs per GPU, "
             "true FP64 residual <= 1e-10")
@@ -281,6 +284,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true",
                     help="skip the plain FP64 GPU solver comparison")
+    ap.add_argument("--no-c5", action="store_true",
+                    help="skip the P->gamma gamma pipeline at 32^3x64")
     ap.add_argument("--ref-niter", type=int, default=0,
                     help="reference arm: iterations per solve given instead of measured "
                          "(0: measured by solving every worker's column first)")
@@ -485,12 +490,57 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         result["cpu_baseline"] = cpu_baseline_leg(result)
 
+    del xs, bs
+    lat.close()
+    if rank == 0 and world == 1 and not args.no_c5:
+        torch.cuda.empty_cache()
+        result["p2gg_c5"] = p2gg_c5_leg(local)
+
     if rank == 0:
         print(json.dumps(result), flush=True)
-    lat.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def p2gg_c5_leg(local):
+    """The P -> gamma gamma pipeline of the 32^3x64 configuration for the
+    first of its four source positions (cvc_b200.p2gg, p2gg_xspace.c:434-899):
+    180 batched mixed-precision solves (both flavours at the source and its
+    four forward neighbours, then the 60 sequential propagators), the
+    sequential sources and the conserved-current contraction, all fields in
+    device memory.  A first pass tunes the solver for this volume; the second
+    is timed (CUDA-synchronised wall time of the whole pipeline)."""
+    import torch
+    import cvc_b200 as cb
+    from cvc_b200 import p2gg as pg
+    lat = cb.Lattice(*C5_DIMS, device=local, kappa=C5_KAPPA, mu=C5_MU2K / (2 * C5_KAPPA),
+                     bc_angle=(1.0, 0.0, 0.0, 0.0))
+    lat.upload_gauge(cb.gauge_random(*C5_DIMS, C5_EPS, C5_SEED))
+    p = cb.solver_defaults()
+    p.precision, p.link_recon, p.tol = cb.PREC_SINGLE, 12, TOL
+    site = pg.source_positions(C5_DIMS, 4, C5_SEED)[0]
+    dev = torch.device("cuda", local)
+    out = {}
+    for rep in range(2):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        conn, contact, st = pg.p2gg(lat, site, C5_DT, (0, 0, 0), 5, 0, p, device=dev)
+        torch.cuda.synchronize()
+        total = time.perf_counter() - t
+        out = {"value": st["solves"] / st["solve_s"], "unit": "solves/s",
+               "seconds_per_source": total, "solves_per_source": st["solves"],
+               "solve_s": st["solve_s"], "contract_s": st["contract_s"],
+               "inner_iterations": st["iterations"], "max_true_residual": st["max_true_res"],
+               "pi_norm": float(torch.linalg.norm(conn)),
+               "workload": "32^3x64 P->gamma gamma, kappa 0.156, 2*kappa*mu 0.004, eps 0.3 "
+                           f"(ranlxd seed 21), source site {site}, sequential source at dt "
+                           f"{C5_DT}, FP32 inner iterations, true FP64 residual <= 1e-10",
+               "passes": rep + 1}
+        del conn
+    lat.close()
+    torch.cuda.empty_cache()
+    return out
 
 
 def cpu_baseline_leg(result):

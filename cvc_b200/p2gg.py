@@ -22,7 +22,8 @@ import time
 
 import numpy as np
 
-from .lattice import Lattice, gauge_random, solver_defaults
+from . import _lib
+from .lattice import CvcbError, Lattice, gauge_random, solver_defaults
 
 
 def shifted_sites(dims, site):
@@ -96,11 +97,19 @@ def p2gg(lat, source_site, dt, momentum, gamma_id, propagator_position=0, params
     solve(up, src, mu if propagator_position == 0 else -mu)
     lat.set_params(kappa, mu, bc)
     del src, b
-    torch.cuda.empty_cache()  # the library allocates with cudaMalloc, outside torch's cache
     conn = torch.zeros(32 * V, dtype=torch.float64, device=device)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    conn, contact = lat.cvc_contract(up + dn, source_site, conn=conn)
+    try:
+        conn, contact = lat.cvc_contract(up + dn, source_site, conn=conn)
+    except CvcbError as e:
+        # the contraction's buffers are allocated by the library (cudaMalloc,
+        # outside torch's cache): give it the memory of the sources that
+        # torch still caches, and try once more
+        if e.code != _lib.CVCB_ERR_NOMEM:
+            raise
+        torch.cuda.empty_cache()
+        conn, contact = lat.cvc_contract(up + dn, source_site, conn=conn)
     torch.cuda.synchronize()
     stats["contract_s"] = time.perf_counter() - t0
     if keep is not None:
