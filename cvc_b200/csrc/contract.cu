@@ -13,8 +13,8 @@
 //   Z_c(x) = sum_{g,ib} conj(k us) chi_{d(g,ir,ib)}(x)
 // after which Pi_mu_nu needs, per column c, one forward and one backward
 // hop of phi_c and two 12-component inner products with Z_c.  Kernel
-// k_cvc_z builds the 24 Z columns of one nu (both parts); k_cvc_pi does the
-// hops and dots, accumulating in FP64 registers.
+// k_cvc_z_sites (or k_cvc_z) builds the 24 Z columns of one nu (both parts);
+// k_cvc_pi does the hops and dots, accumulating in FP64 registers.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -52,6 +52,39 @@ __global__ void __launch_bounds__(128) k_cvc_z(double2 *__restrict__ Z,
     double2 *z = Z + col * fs;
 #pragma unroll
     for (int k = 0; k < 12; ++k) z[(size_t)k * V + s] = make_double2(acc[k].re, acc[k].im);
+  }
+}
+
+// The same Z columns with each dn column that one nu needs read once per
+// site: thread = (site, spinor component k = blockIdx.y).  Its inputs (at
+// most 24 columns) are staged in shared memory, because the plan picks them
+// at run time, and every output is formed with the same terms in the same
+// order as k_cvc_z (the same bits).  k_cvc_z reads 6 inputs per output
+// column, 144 field reads per nu, most of them from L2 or DRAM again.
+constexpr int kZThreads = 128;
+struct ZPlanLocal {
+  double2 coef[24][6];
+  int field[24];             // dn column (0..59) of local input f
+  unsigned char loc[24][6];  // local input of term q of output column col
+  int nin;                   // local inputs in use
+};
+
+__global__ void __launch_bounds__(kZThreads) k_cvc_z_sites(double2 *__restrict__ Z,
+                                                          const double2 *__restrict__ dn,
+                                                          ZPlanLocal plan, int V) {
+  __shared__ double2 in[24][kZThreads];
+  const int s = blockIdx.x * kZThreads + threadIdx.x;
+  if (s >= V) return;  // each thread reads only its own slots: no barrier below
+  const size_t fs = (size_t)12 * V, off = (size_t)blockIdx.y * V + s;
+  for (int f = 0; f < plan.nin; ++f) in[f][threadIdx.x] = __ldg(dn + plan.field[f] * fs + off);
+  for (int col = 0; col < 24; ++col) {
+    Cx<double> acc = cx(0.0, 0.0);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const double2 v = in[plan.loc[col][q]][threadIdx.x];
+      cfma(acc, cx(plan.coef[col][q].x, plan.coef[col][q].y), cx(v.x, v.y));
+    }
+    Z[col * fs + off] = make_double2(acc.re, acc.im);
   }
 }
 
@@ -325,9 +358,33 @@ int make_zplans(cvcb_lattice *L, int src, ZPlan plans[4], double Us[4][18], ZMet
   return CVCB_OK;
 }
 
-// Z columns of one nu into Z (24 fields), from the 60 dn fields at dn.
+// Z columns of one nu into Z (24 fields), from the 60 dn fields at dn:
+// k_cvc_z_sites when the plan draws on at most 24 distinct dn columns (one
+// nu: the 12 shifted by nu and the 12 unshifted ones), else k_cvc_z.
 int launch_cvc_z(cvcb_lattice *L, double2 *Z, const double2 *dn, const ZPlan &plan) {
-  k_cvc_z<<<(L->g.V + 127) / 128, 128, 0, L->stream>>>(Z, dn, plan, L->g.V);
+  ZPlanLocal lp{};
+  bool fits = true;
+  for (int col = 0; col < 24 && fits; ++col)
+    for (int q = 0; q < 6 && fits; ++q) {
+      const int src = plan.t[col][q].src;
+      int f = 0;
+      while (f < lp.nin && lp.field[f] != src) ++f;
+      if (f == lp.nin) {
+        if (lp.nin == 24) {
+          fits = false;
+          break;
+        }
+        lp.field[lp.nin++] = src;
+      }
+      lp.loc[col][q] = (unsigned char)f;
+      lp.coef[col][q] = plan.t[col][q].coef;
+    }
+  if (fits) {
+    dim3 grid((L->g.V + kZThreads - 1) / kZThreads, 12);
+    k_cvc_z_sites<<<grid, kZThreads, 0, L->stream>>>(Z, dn, lp, L->g.V);
+  } else {
+    k_cvc_z<<<(L->g.V + 127) / 128, 128, 0, L->stream>>>(Z, dn, plan, L->g.V);
+  }
   CVCB_LAUNCHED(L);
   return CVCB_OK;
 }
@@ -385,9 +442,7 @@ int cvc_contract(cvcb_lattice *L, const double *const *fields, int src, double *
     }
   };
   for (int nu = 0; nu < 4; ++nu) {
-    const ZPlan &plan = plans[nu];
-    k_cvc_z<<<blocks, 128, 0, L->stream>>>(static_cast<double2 *>(zb), P + 60 * fs, plan, g.V);
-    CVCB_LAUNCHED(L);
+    CVCB_TRY(launch_cvc_z(L, static_cast<double2 *>(zb), P + 60 * fs, plans[nu]));
     if (g_cvc_pi_variant < 0) {  // first use in this process: time the variants (same results)
       cudaEvent_t e0, e1;
       CVCB_CUDA(cudaEventCreate(&e0));
