@@ -2,17 +2,17 @@
 // batched solver.
 //
 // Right-hand sides 2q and 2q+1 ("pair q") are stored interleaved per complex
-// spin-colour component, so that one 16-byte load yields both right-hand
-// sides of a component in the register order of the packed FP32x2
-// instructions (FFMA2/FADD2/FMUL2):
-//   float4 P[pair][tile = j / 32][component k = 0..11][j % 32]
+// spin-colour component, so that 16 bytes hold both right-hand sides of a
+// component in the register order of the packed FP32x2 instructions
+// (FFMA2/FADD2/FMUL2), and two components of a site are adjacent:
+//   float4 P[pair][tile = j / 32][component pair k / 2][j % 32][k % 2]
 //   float4 = (re of rhs 2q, re of rhs 2q+1, im of rhs 2q, im of rhs 2q+1)
-// A warp reading component k of 32 consecutive sites reads 512 contiguous
-// bytes; the 12 components of one site lie at fixed offsets (k * 512 B) from
-// one address, so a neighbour costs one address computation, not twelve.
-// Links are tiled the same way (tile = even/odd link index / 32), with 18
-// reals (phase multiplied in; nothing to rebuild) or 12 reals (rows 0, 1;
-// row 2 rebuilt in registers).
+// One 256-bit load per thread reads components 2m and 2m+1 of its site; a
+// warp reads 1 KB contiguous; the 6 component pairs of a site lie at fixed
+// offsets (m * 1 KB) from one address, so a neighbour costs one address
+// computation and six loads.  Links are tiled by 32 even/odd link indices
+// too, with 18 reals (phase multiplied in; nothing to rebuild) or 12 reals
+// (rows 0, 1; row 2 rebuilt in registers).
 //
 // Compared with per-rhs structure-of-arrays storage packed into FP32x2 pairs
 // after the loads (k_eo_hop_x2), the stencil needs no register moves to form
@@ -36,25 +36,56 @@ __device__ __forceinline__ float4 f4_of(const CP &c) {
   return make_float4(c.re.x, c.re.y, c.im.x, c.im.y);
 }
 
-// FP32 pair-tiled field set: pair pr, half-lattice site j.
+// 256-bit global accesses (sm_100): two float4 from 32-byte-aligned
+// addresses in one instruction.  The asm statements are volatile with a
+// memory clobber so that the compiler keeps them in order with the other
+// memory accesses of the thread (a field is often read and then written by
+// the same thread).
+__device__ __forceinline__ void ldg_v8(const float4 *q, float4 &a, float4 &b) {
+  asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z),
+                 "=f"(b.w)
+               : "l"(q)
+               : "memory");
+}
+__device__ __forceinline__ void stg_v8(float4 *q, const float4 &a, const float4 &b) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(q), "f"(a.x),
+               "f"(a.y), "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+               : "memory");
+}
+
+// FP32 pair-tiled field set: pair pr, half-lattice site j.  Within a tile of
+// 32 sites, component k of the site in position l sits at float4
+// comp(k) + 2 l = (k / 2) * 64 + k % 2 + 2 l: components 2m and 2m + 1 of a
+// site are 32 contiguous bytes, read or written with one 256-bit access
+// (a warp: 1 KB contiguous), six per site and rhs pair.
 struct P32 {
   using R = float;
   float4 *p;
   size_t pstride;  // float4 per pair (tiles x 12 x 32)
+  __device__ __forceinline__ static constexpr int comp(int k) { return (k >> 1) * (2 * kTile) + (k & 1); }
+  // the site's slot: component k at at(pr, j) + comp(k)
   __device__ __forceinline__ float4 *at(int pr, int j) const {
-    return p + (size_t)pr * pstride + (size_t)(j >> 5) * (12 * kTile) + (j & (kTile - 1));
+    return p + (size_t)pr * pstride + (size_t)(j >> 5) * (12 * kTile) + 2 * (j & (kTile - 1));
   }
   __device__ __forceinline__ SpinorPair load_pair(int pr, int j) const {
     const float4 *q = at(pr, j);
     SpinorPair s;
 #pragma unroll
-    for (int k = 0; k < 12; ++k) s.c[k / 3][k % 3] = cp_of(__ldg(q + k * kTile));
+    for (int m = 0; m < 6; ++m) {
+      float4 a, b;
+      ldg_v8(q + m * 2 * kTile, a, b);
+      s.c[(2 * m) / 3][(2 * m) % 3] = cp_of(a);
+      s.c[(2 * m + 1) / 3][(2 * m + 1) % 3] = cp_of(b);
+    }
     return s;
   }
   __device__ __forceinline__ void store_pair(int pr, int j, const SpinorPair &s) const {
     float4 *q = at(pr, j);
 #pragma unroll
-    for (int k = 0; k < 12; ++k) q[k * kTile] = f4_of(s.c[k / 3][k % 3]);
+    for (int m = 0; m < 6; ++m)
+      stg_v8(q + m * 2 * kTile, f4_of(s.c[(2 * m) / 3][(2 * m) % 3]),
+             f4_of(s.c[(2 * m + 1) / 3][(2 * m + 1) % 3]));
   }
   // one lane of a pair (lane 0: rhs 2 pr, lane 1: rhs 2 pr + 1); the other
   // lane's values are left as they are
@@ -63,8 +94,8 @@ struct P32 {
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
       const CP &c = s.c[k / 3][k % 3];
-      q[4 * kTile * k] = lane ? c.re.y : c.re.x;
-      q[4 * kTile * k + 2] = lane ? c.im.y : c.im.x;
+      q[4 * comp(k)] = lane ? c.re.y : c.re.x;
+      q[4 * comp(k) + 2] = lane ? c.im.y : c.im.x;
     }
   }
   // per-rhs access (for the kernels that run once per reliable update)
@@ -73,9 +104,12 @@ struct P32 {
     const bool b = r & 1;
     Spinor<float> s;
 #pragma unroll
-    for (int k = 0; k < 12; ++k) {
-      const float4 v = __ldg(q + k * kTile);
-      s.c[k / 3][k % 3] = cx(b ? v.y : v.x, b ? v.w : v.z);
+    for (int m = 0; m < 6; ++m) {
+      float4 v[2];
+      ldg_v8(q + m * 2 * kTile, v[0], v[1]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        s.c[(2 * m + h) / 3][(2 * m + h) % 3] = cx(b ? v[h].y : v[h].x, b ? v[h].w : v[h].z);
     }
     return s;
   }
@@ -87,8 +121,8 @@ struct P32 {
     float *q = reinterpret_cast<float *>(at(r >> 1, j)) + (r & 1);
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-      q[4 * kTile * k] = s.c[k / 3][k % 3].re;
-      q[4 * kTile * k + 2] = s.c[k / 3][k % 3].im;
+      q[4 * comp(k)] = s.c[k / 3][k % 3].re;
+      q[4 * comp(k) + 2] = s.c[k / 3][k % 3].im;
     }
   }
 };
@@ -597,9 +631,9 @@ __global__ void __launch_bounds__(kTmemThreads, PIPE ? 4 : 6) k_eo_hop_ptm(HopAr
         x.re = make_float2(v[4 * kk], v[4 * kk + 1]);
         x.im = make_float2(v[4 * kk + 2], v[4 * kk + 3]);
         CP o = diag_comp(x, (float)(A.c * A.d1a) * gh, (float)(A.c * A.d1b) * g5 * gh);
-        if (AUX) diag_comp_acc(o, cp_of(__ldg(auxp + k * kTile)), (float)A.d2a, (float)A.d2b * g5);
+        if (AUX) diag_comp_acc(o, cp_of(__ldg(auxp + P32::comp(k))), (float)A.d2a, (float)A.d2b * g5);
         if (RUPD) {
-          CP rv = cp_of(__ldg(dst + k * kTile));
+          CP rv = cp_of(__ldg(dst + P32::comp(k)));
           rv.re = __ffma2_rn(na, o.re, rv.re);
           rv.im = __ffma2_rn(na, o.im, rv.im);
           o = rv;
@@ -612,9 +646,9 @@ __global__ void __launch_bounds__(kTmemThreads, PIPE ? 4 : 6) k_eo_hop_ptm(HopAr
             n2.y = fma((double)o.im.y, (double)o.im.y, n2.y);
           }
           if (act_a && act_b) {
-            dst[k * kTile] = f4_of(o);
+            dst[P32::comp(k)] = f4_of(o);
           } else {
-            float *qf = reinterpret_cast<float *>(dst + k * kTile) + (act_a ? 0 : 1);
+            float *qf = reinterpret_cast<float *>(dst + P32::comp(k)) + (act_a ? 0 : 1);
             qf[0] = act_a ? o.re.x : o.re.y;
             qf[2] = act_a ? o.im.x : o.im.y;
           }
@@ -701,7 +735,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
 __device__ __forceinline__ SpinorPair stage_load(const float4 *S, int lane) {
   SpinorPair f;
 #pragma unroll
-  for (int k = 0; k < 12; ++k) f.c[k / 3][k % 3] = cp_of(S[k * kTile + lane]);
+  for (int k = 0; k < 12; ++k) f.c[k / 3][k % 3] = cp_of(S[P32::comp(k) + 2 * lane]);
   return f;
 }
 
