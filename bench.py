@@ -494,7 +494,11 @@ def main():
     lat.close()
     if rank == 0 and world == 1 and not args.no_c5:
         torch.cuda.empty_cache()
-        result["p2gg_c5"] = p2gg_c5_leg(local)
+        try:
+            result["p2gg_c5"] = p2gg_c5_leg(local)
+        except Exception as e:  # an extra figure: its failure must not cost the headline line
+            result["p2gg_c5"] = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+            torch.cuda.empty_cache()
 
     if rank == 0:
         print(json.dumps(result), flush=True)
