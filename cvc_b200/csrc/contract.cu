@@ -16,6 +16,7 @@
 // k_cvc_z_sites (or k_cvc_z) builds the 24 Z columns of one nu (both parts);
 // k_cvc_pi does the hops and dots, accumulating in FP64 registers.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -166,6 +167,48 @@ __global__ void __launch_bounds__(128, MINB) k_cvc_pi(double *__restrict__ conn,
     o[2 * (4 * mu + nu)] = -0.25 * pi[mu].re;  // normalisation, :861
     o[2 * (4 * mu + nu) + 1] = -0.25 * pi[mu].im;
   }
+}
+
+// The same Pi_mu_nu with one thread per (site, mu), mu = blockIdx.y: four
+// times the threads, each with one link and a quarter of the loop (no
+// unrolled mu loop holding its state), so that more warps fit under the
+// same register cap.  Each thread accumulates pi_mu over (part, c) in the
+// order of k_cvc_pi and writes only its own mu entry: the same bits.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_cvc_pi_mu(double *__restrict__ conn,
+                                                   const double2 *__restrict__ P0,
+                                                   const double2 *__restrict__ P1,
+                                                   const double2 *__restrict__ Z,
+                                                   const double2 *__restrict__ U, Geom g, int nu) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= g.V) return;
+  const int mu = blockIdx.y;
+  const int p = s >= g.Vh;
+  const SiteCoord cd = site_coord(g, p, s - p * g.Vh);
+  const size_t V = g.V, fs = (size_t)12 * V;
+  const int j = (1 - p) * g.Vh + (nb_lex(g, cd, mu, +1) >> 1);
+  const Link<double> W = load_link64(U, V, mu, s);
+  Cx<double> pi = cx(0.0, 0.0);
+  for (int part = 0; part < 2; ++part) {
+    const double2 *P = part == 0 ? P0 : P1;
+    for (int c = 0; c < 12; ++c) {
+      const double2 *Pc = P + c * fs;
+      const double2 *Zc = Z + (part * 12 + c) * fs;
+      {  // forward: g5 (g_mu - 1) U_mu(x) P_c(x+mu), dotted with Z_c(x)
+        const HalfSpinor<double> h = project(mu, -1, load_spinor(Pc, V, j));
+        const Spinor<double> r = recon_full(mu, -1, link_mul(W, h));
+        pi = pi - dot_g5(load_spinor(Zc, V, s), r);
+      }
+      {  // backward: g5 (g_mu + 1) U_mu(x)^+ P_c(x), dotted with Z_c(x+mu)
+        const HalfSpinor<double> h = project(mu, +1, load_spinor(Pc, V, s));
+        const Spinor<double> r = recon_full(mu, +1, link_dag_mul(W, h));
+        pi = pi + dot_g5(load_spinor(Zc, V, j), r);
+      }
+    }
+  }
+  double *o = conn + (size_t)cd.lex * 32;
+  o[2 * (4 * mu + nu)] = -0.25 * pi.re;  // normalisation, :861
+  o[2 * (4 * mu + nu) + 1] = -0.25 * pi.im;
 }
 
 // Ward identity divergence on the CVC-layout conn (cvc_exact2_xspace.c:938-953)
@@ -403,6 +446,8 @@ static int conn_out(cvcb_lattice *L, double *dst, const double *src, size_t ndou
   return CVCB_OK;
 }
 
+// Variant of the Pi kernel (0-2: k_cvc_pi at 2, 3, 4 blocks per SM; 3-5:
+// k_cvc_pi_mu likewise), timed on first use; CVCB_CVC_PI=v pins it.
 static int g_cvc_pi_variant = -1;
 
 int cvc_contract(cvcb_lattice *L, const double *const *fields, int src, double *conn,
@@ -435,20 +480,29 @@ int cvc_contract(cvcb_lattice *L, const double *const *fields, int src, double *
   auto pi = [&](int v, int nu) {
     double *c = static_cast<double *>(cb);
     const double2 *P1 = P + (size_t)nu * 12 * fs, *Z = static_cast<const double2 *>(zb);
+    const dim3 gmu(blocks, 4);  // k_cvc_pi_mu: one thread per (site, mu)
     switch (v) {
       case 1: k_cvc_pi<3><<<blocks, 128, 0, L->stream>>>(c, P + 48 * fs, P1, Z, L->U64, g, nu); break;
       case 2: k_cvc_pi<4><<<blocks, 128, 0, L->stream>>>(c, P + 48 * fs, P1, Z, L->U64, g, nu); break;
+      case 3: k_cvc_pi_mu<2><<<gmu, 128, 0, L->stream>>>(c, P + 48 * fs, P1, Z, L->U64, g, nu); break;
+      case 4: k_cvc_pi_mu<3><<<gmu, 128, 0, L->stream>>>(c, P + 48 * fs, P1, Z, L->U64, g, nu); break;
+      case 5: k_cvc_pi_mu<4><<<gmu, 128, 0, L->stream>>>(c, P + 48 * fs, P1, Z, L->U64, g, nu); break;
       default: k_cvc_pi<2><<<blocks, 128, 0, L->stream>>>(c, P + 48 * fs, P1, Z, L->U64, g, nu); break;
     }
   };
   for (int nu = 0; nu < 4; ++nu) {
     CVCB_TRY(launch_cvc_z(L, static_cast<double2 *>(zb), P + 60 * fs, plans[nu]));
+    if (g_cvc_pi_variant < 0)
+      if (const char *env = getenv("CVCB_CVC_PI")) {
+        const int v = atoi(env);
+        if (v >= 0 && v < 6) g_cvc_pi_variant = v;
+      }
     if (g_cvc_pi_variant < 0) {  // first use in this process: time the variants (same results)
       cudaEvent_t e0, e1;
       CVCB_CUDA(cudaEventCreate(&e0));
       CVCB_CUDA(cudaEventCreate(&e1));
       float best = 1e30f;
-      for (int v = 0; v < 3; ++v) {
+      for (int v = 0; v < 6; ++v) {
         CVCB_CUDA(cudaEventRecord(e0, L->stream));
         pi(v, nu);
         CVCB_CUDA(cudaEventRecord(e1, L->stream));

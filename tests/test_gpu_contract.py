@@ -91,3 +91,41 @@ def test_seq_source(env, t, mom, gid, pos):
     lat.p2gg_seq_source(src, prop, t, mom, gid, pos)
     ref = orc.seq_source(prop, t, mom, gid, pos)
     assert rel_err(src, ref) < 1e-14
+
+
+VARIANT_CHILD = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+sys.path.insert(0, sys.argv[1] + "/tests")
+import cvc_b200 as cb
+from conftest import seeded
+dims = (8, 4, 4, 6)
+lat = cb.Lattice(*dims, kappa=0.15, mu=0.01 / 0.3)
+lat.upload_gauge(cb.gauge_random(*dims, 0.3, 1234))
+V = lat.VOLUME
+fields = [seeded(3000 + i, 24 * V) for i in range(120)]
+conn, contact = lat.cvc_contract(fields, 41)
+np.save(sys.argv[2], conn)
+"""
+
+
+def test_pi_kernel_variants_agree(tmp_path):
+    """Every Pi kernel the contraction times on first use (one thread per
+    site at three register caps, one thread per site and mu at three),
+    pinned by CVCB_CVC_PI in a child process: the same Pi to the last bit
+    (the same terms, accumulated in the same order)."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    out = {}
+    for v in range(6):
+        f = tmp_path / f"pi{v}.npy"
+        env = dict(os.environ, CVCB_CVC_PI=str(v))
+        r = subprocess.run([sys.executable, "-c", VARIANT_CHILD, str(ROOT), str(f)], env=env,
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[v] = np.load(f)
+    for v in range(1, 6):
+        assert np.array_equal(out[v], out[0]), (v, float(np.max(np.abs(out[v] - out[0]))))
